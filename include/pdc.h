@@ -1,0 +1,216 @@
+/*
+ * pdc.h -- C ABI of the B200 primal-dual interior-point contact solver.
+ *
+ * This is the drop-in boundary for the reference's force-solver interface
+ *   virtual void ForceSolver::fillForces(const FloatType timestep,
+ *       const Vector3& gravity, std::vector<ContactInformation>& contactInfo,
+ *       std::vector<std::unique_ptr<RigidObjectBase>>& objects) = 0;
+ * (src/Solver/ForceSolverBase.h:78-82), implemented there by
+ * PrimalDualForceSolver::fillForces (src/Solver/PrimalDual/PrimalDualForceSolver.cpp:79-130).
+ *
+ * Everything here is plain C: pointers, sizes and int status codes.  No
+ * exception crosses this boundary.  Host arrays are owned by the caller; device
+ * buffers are owned by the solver handle and reused across steps.  One handle
+ * per host thread.
+ *
+ * Data layout (structure of arrays, all double precision, row-major):
+ *   body b:     vel[3b..3b+2], ang_vel[3b..], mass[b],
+ *               inertia[6b..6b+5]      world-frame inertia  (xx,yy,zz,xy,xz,yz)
+ *               inv_inertia[6b..6b+5]  world-frame inverse inertia, same order
+ *               is_static[b]           1 = prescribed motion (RigidObjectBase::isStatic)
+ *   contact c:  body[2c], body[2c+1]   ids of objId[0], objId[1]
+ *               frame[9c..9c+8]        3x3 contact frame R, row-major; column 0 is the
+ *                                      normal n, columns 1,2 the tangents t1,t2
+ *                                      (= ContactInformation::transformation[0].topRows(3))
+ *               arm[6c..6c+5]          lever arms c0 = pos - x(body0), c1 = pos - x(body1)
+ *               depth[c]               penetration depth (ContactInformation::depth)
+ *               mu[c]                  optional per-contact friction coefficient (NULL:
+ *                                      the config's single global coefficient, as in the
+ *                                      reference)
+ * The per-body Jacobian blocks of the reference,
+ *   transformation[0] = [R; c0 x R],  transformation[1] = -[R; c1 x R]
+ * (src/Contact/ContactGenerator/ContactGeneratorBase.h:21-49), are rebuilt from
+ * (R, c0, c1) on the device.
+ */
+#ifndef PDC_H
+#define PDC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDC_ABI_VERSION 1
+
+/* Call status codes. */
+enum pdc_status {
+    PDC_OK = 0,
+    PDC_EINVAL = 1,   /* bad argument or configuration (reference: std::runtime_error) */
+    PDC_ECUDA = 2,    /* a CUDA runtime call failed */
+    PDC_ENOMEM = 3,   /* device allocation failed */
+    PDC_ETIMEOUT = 4, /* a bounded device wait ran out */
+    PDC_ENODEV = 5    /* no CUDA device / extension unusable */
+};
+
+/* Per-scene convergence status: returned as data, never as an error, the way the
+ * reference degrades silently (PrimalDualForceSolver.cpp:390-394, 444-467, 488). */
+enum pdc_scene_status {
+    PDC_SCENE_OK = 0,        /* exitErr < tolerance */
+    PDC_SCENE_MAX_ITER = 1,  /* Newton loop hit solver.iterations */
+    PDC_SCENE_LS_FAIL = 2,   /* at least one Newton and gradient step were both rejected */
+    PDC_SCENE_NONFINITE = 4, /* a non-finite value appeared; the linear step fell back to 0 */
+    PDC_SCENE_TIMEOUT = 8    /* a device-side iteration cap other than Newton's was hit */
+};
+
+enum pdc_force_model {
+    PDC_FORCE_NON_SMOOTH_CONTACT = 0, /* non_smooth_force.name: non_smooth_contact */
+    PDC_FORCE_ONLY_NORMAL = 1         /* non_smooth_force.name: only_normal */
+};
+
+enum pdc_precision {
+    PDC_PRECISION_FP64 = 0,  /* plain FP64 everywhere */
+    PDC_PRECISION_MIXED = 1  /* FP32 bulk (contact terms, PCG) + FP64 refinement/merit */
+};
+
+/* Solver configuration.  Defaults (pdc_config_default) are the reference's YAML
+ * defaults: PrimalDualForceSolver.cpp:650-652, NonSmoothContactForce.cpp:320-334. */
+typedef struct pdc_config {
+    int32_t abi_version;      /* must be PDC_ABI_VERSION */
+    int32_t max_iter;         /* solver.iterations (100) */
+    double tol;               /* solver.tolerance (1e-6) */
+    int32_t force_model;      /* enum pdc_force_model */
+    int32_t spring_based;     /* non_smooth_force.spring_based_force (0) */
+    double mu;                /* non_smooth_force.static_coeff (0.5) */
+    double restitution;       /* non_smooth_force.restitution (0.0; only_normal: 0.5) */
+    double spring_k;          /* non_smooth_force.spring_k (1e6) */
+    double spring_damp;       /* non_smooth_force.spring_damp (0.01) */
+    int32_t precision;        /* enum pdc_precision */
+    int32_t direct_threshold; /* local bodies below this use the direct-solve branch (2000) */
+    double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
+    int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
+    double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */
+    int32_t pcg_max_iter;     /* iteration cap of the iterative branch (1000, :381) */
+    double mixed_inner_rtol;  /* FP32 inner PCG relative residual (mixed precision) */
+    int32_t warm_start;       /* 0: cold start every step, as the reference (:269) */
+    int32_t device;           /* CUDA device ordinal */
+} pdc_config;
+
+/* Body state (input).  See the layout note at the top of this file. */
+typedef struct pdc_bodies_soa {
+    int32_t n;
+    const double* vel;
+    const double* ang_vel;
+    const double* mass;
+    const double* inertia;
+    const double* inv_inertia;
+    const uint8_t* is_static;
+} pdc_bodies_soa;
+
+/* Contact set (input). */
+typedef struct pdc_contacts_soa {
+    int32_t n;
+    const int32_t* body;
+    const double* frame;
+    const double* arm;
+    const double* depth;
+    const double* mu; /* may be NULL */
+} pdc_contacts_soa;
+
+/* Per-solve diagnostics (KKT parts are in the solver's non-dimensional units). */
+typedef struct pdc_stats {
+    int32_t status;         /* bit set of enum pdc_scene_status */
+    int32_t newton_iters;   /* itCoupled (:488) */
+    int32_t pcg_iters;      /* total linear iterations */
+    int32_t ls_trials;      /* total line-search trials */
+    int32_t gd_fallbacks;   /* gradient-descent fallbacks (:444-467) */
+    int32_t n_local_bodies; /* bodies in contact (:96-111) */
+    double exit_err;        /* exitErr at exit (:302-307) */
+    double kkt_stationarity;/* max(|ru|/6N_b, |rf|/3N_c) */
+    double kkt_complementarity; /* max(|lambda.c|_inf, dual gap) */
+    double kkt_cone;        /* max over contacts of max(0, c_cone(f), -f_n) */
+    double char_mass;       /* charMass (:23-78) */
+    double char_speed;      /* charSpeed (:23-78) */
+} pdc_stats;
+
+/* Results (output).  dvel/dang_vel = RigidObjectBase::acceleration()/angularAcc(),
+ * i.e. velocity increments, for EVERY body (g*dt for bodies not in contact);
+ * local_force = ContactInformation::localForce (impulse in the (n,t1,t2) frame). */
+typedef struct pdc_result {
+    double* dvel;         /* [n_bodies][3] */
+    double* dang_vel;     /* [n_bodies][3] */
+    double* local_force;  /* [n_contacts][3] */
+    pdc_stats stats;
+} pdc_result;
+
+typedef struct pdc_solver pdc_solver;
+
+/* Fill a config with the reference defaults. */
+void pdc_config_default(pdc_config* cfg);
+
+/* Create / destroy a solver handle (PrimalDualForceSolver + fillFromYAML). */
+int pdc_create(const pdc_config* cfg, pdc_solver** out);
+void pdc_destroy(pdc_solver* s);
+
+/* Reset timers and iteration counters (ForceSolver::reset, ForceSolverBase.h:67). */
+int pdc_reset(pdc_solver* s);
+
+/* Solve one step, synchronously (ForceSolver::fillForces, ForceSolverBase.h:78-82).
+ * Host arrays in, host arrays out.  Contacts with no bodies in them are an error;
+ * zero contacts returns dvel = g*dt for every body (PrimalDualForceSolver.cpp:85-93). */
+int pdc_solve(pdc_solver* s, double dt, const double gravity[3],
+              const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
+              pdc_result* out);
+
+/* Same as pdc_solve but every pointer in bodies/contacts/out is a DEVICE pointer
+ * and the work is enqueued on `stream` (a cudaStream_t; NULL = legacy stream).
+ * out->stats is filled when the stream is synchronized via pdc_sync. */
+int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3],
+                    const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
+                    pdc_result* out, void* stream);
+
+/* Batched solve: n_scenes independent scenes packed as ragged CSR.  Scene k owns
+ * bodies [body_offsets[k], body_offsets[k+1]) and contacts
+ * [contact_offsets[k], contact_offsets[k+1]); contact body ids are LOCAL to the
+ * scene (0 .. n_bodies_k-1).  Each scene is the same computation as one
+ * pdc_solve call on that scene alone. */
+typedef struct pdc_batch {
+    int32_t n_scenes;
+    const int32_t* body_offsets;    /* [n_scenes+1] */
+    const int32_t* contact_offsets; /* [n_scenes+1] */
+    const double* dt;               /* [n_scenes] time step per scene */
+    const double* gravity;          /* [n_scenes][3] */
+} pdc_batch;
+
+/* Host arrays; stats has n_scenes entries. */
+int pdc_batch_solve(pdc_solver* s, const pdc_batch* batch,
+                    const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
+                    double* dvel, double* dang_vel, double* local_force,
+                    pdc_stats* stats);
+
+/* Device arrays (batch offsets/dt/gravity too); enqueued on `stream`.
+ * stats (device, n_scenes entries) may be NULL. */
+int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
+                          const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
+                          double* dvel, double* dang_vel, double* local_force,
+                          pdc_stats* stats, void* stream);
+
+/* Wait for the handle's outstanding work (bounded: PDC_ETIMEOUT after timeout_ms). */
+int pdc_sync(pdc_solver* s, int32_t timeout_ms);
+
+/* Accumulated timings (PrimalDualForceSolver::printTimings, :636-648): seconds of
+ * device time in [0] total force calc, [1] build system, [2] solve system,
+ * [3] line search, and [4] total Newton iterations, [5] solves. */
+int pdc_timings(pdc_solver* s, double out[6]);
+
+/* Last error message of this handle (or of the last failed pdc_create if s is NULL). */
+const char* pdc_last_error(const pdc_solver* s);
+
+/* Library version string. */
+const char* pdc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDC_H */
