@@ -88,6 +88,8 @@ typedef struct pdc_config {
     double spring_damp;       /* non_smooth_force.spring_damp (0.01) */
     int32_t precision;        /* enum pdc_precision */
     int32_t direct_threshold; /* local bodies below this use the direct-solve branch (2000) */
+    int32_t dense_max_bodies; /* direct branch: dense Cholesky on the device up to this many
+                                 active bodies (64); larger scenes use PCG */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
     int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
     double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */

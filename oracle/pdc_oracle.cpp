@@ -34,6 +34,7 @@
 // initial guess and Hu rule (:395-427, :474-479).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <set>
@@ -483,6 +484,12 @@ static void reserve_system(const Problem& P, BlockSystem& S) {
     S.A.assign(S.blk_col.size() * 36, 0.0);
     // ordering + scalar upper CSC of the permuted matrix
     S.perm = min_degree_order(S.nbr);
+    if (std::getenv("PDC_ORACLE_NATURAL_ORDER")) {  // sensitivity checks: identity ordering
+        for (int k = 0; k < P.nl; ++k) S.perm[k] = k;
+    }
+    if (std::getenv("PDC_ORACLE_REVERSE_ORDER")) {  // sensitivity checks: reversed ordering
+        std::reverse(S.perm.begin(), S.perm.end());
+    }
     S.iperm.assign(P.nl, 0);
     for (int k = 0; k < P.nl; ++k) S.iperm[S.perm[k]] = k;
     const int n = 6 * P.nl;
@@ -912,6 +919,13 @@ static void fill_forces_intl(Problem& P, pdc_stats* st) {
                 S.ldlt.solve(x);
                 for (int bk = 0; bk < nl; ++bk)
                     for (int r = 0; r < 6; ++r) du[6 * S.perm[bk] + r] = x[6 * bk + r];
+                if (std::getenv("PDC_ORACLE_CHECK_SOLVE")) {  // debugging aid: solve residual
+                    std::vector<Real> q;
+                    block_matvec(S, du, q, 1);
+                    Real rn = 0, bn = 0;
+                    for (size_t k = 0; k < n_rigid; ++k) { rn += (q[k] - rhs[k]) * (q[k] - rhs[k]); bn += rhs[k] * rhs[k]; }
+                    std::fprintf(stderr, "it %d eps %.3e relres %.3e\n", it, eps, std::sqrt(rn / bn));
+                }
             } else {
                 std::fill(du.begin(), du.end(), 0.0);
                 P.nonfinite = true;
@@ -927,6 +941,12 @@ static void fill_forces_intl(Problem& P, pdc_stats* st) {
             P.pcg_total += (int)iters;
         }
         for (size_t q = 0; q < n_rigid; ++q) du[q] = du[q] * D[q];
+        if (const char* pe = std::getenv("PDC_ORACLE_PERTURB")) {
+            // sensitivity checks only: relative perturbation of the Newton
+            // direction at round-off level (deterministic sign pattern)
+            const Real eps_p = std::atof(pe);
+            for (size_t q = 0; q < n_rigid; ++q) du[q] *= 1.0 + eps_p * ((((q * 2654435761u) >> 7) & 1) ? 1.0 : -1.0);
+        }
 
         // retrieveNonSmoothForceInc (NonSmoothContactForce.cpp:254-280 / OnlyNormalForce.cpp:152-171)
         df.assign(n_force, 0.0);
@@ -968,6 +988,9 @@ static void fill_forces_intl(Problem& P, pdc_stats* st) {
         P.vels = ls.u;
         P.forces = ls.f;
         P.lambda = ls.l;
+        if (std::getenv("PDC_ORACLE_TRACE"))  // debugging aid: per-iteration scalars
+            std::fprintf(stderr, "it %d err %.17e eps %.17e step %.17e gd %d |du| %.17e\n", it, err, eps, ls.step,
+                         (int)useGD, std::sqrt(dotv(du, du)));
         if (!useGD && ls.step == 1) {
             if (iters == maxCGIt && !direct) Hu *= 1.3;
             else Hu /= 4;

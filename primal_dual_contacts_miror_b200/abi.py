@@ -42,6 +42,7 @@ class Config(C.Structure):
         ("spring_damp", C.c_double),
         ("precision", C.c_int32),
         ("direct_threshold", C.c_int32),
+        ("dense_max_bodies", C.c_int32),
         ("pcg_rtol_direct", C.c_double),
         ("pcg_max_direct", C.c_int32),
         ("pcg_rtol_iter", C.c_double),
@@ -129,6 +130,7 @@ def default_config(**overrides):
     cfg.spring_damp = 0.01
     cfg.precision = PDC_PRECISION_FP64
     cfg.direct_threshold = 2000
+    cfg.dense_max_bodies = 64
     cfg.pcg_rtol_direct = 1e-13
     cfg.pcg_max_direct = 4000
     cfg.pcg_rtol_iter = 1e-8

@@ -1,0 +1,494 @@
+// C ABI of the B200 contact solver (include/pdc.h).
+//
+// A handle owns one CUDA stream and one device arena that grows on demand and
+// is reused across steps.  pdc_solve / pdc_batch_solve copy host arrays in and
+// results out around one batched kernel launch; the *_async variants take
+// device pointers and only enqueue work.
+#include <cuda_runtime.h>
+#include <time.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/pdc.h"
+#include "pdc_engine.cuh"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Arena {
+    void* base = nullptr;
+    size_t cap = 0;
+    size_t off = 0;
+    void reset() { off = 0; }
+    template <typename T>
+    T* take(size_t n) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(static_cast<char*>(base) + off);
+        off += n * sizeof(T);
+        return p;
+    }
+};
+
+}  // namespace
+
+struct pdc_solver {
+    pdc_config cfg;
+    int device = 0;
+    int num_sms = 0;
+    int blocks_per_sm = 1;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    std::string err;
+    // host-side accumulated statistics (printTimings)
+    double t_total = 0, t_build = 0, t_solve = 0, t_ls = 0;
+    long long newton_total = 0, solves = 0;
+    unsigned long long* d_timers = nullptr;
+    int* d_counter = nullptr;
+};
+
+static int fail(pdc_solver* s, int code, const std::string& msg) {
+    if (s) s->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+static int cuda_fail(pdc_solver* s, cudaError_t e, const char* what) {
+    return fail(s, e == cudaErrorMemoryAllocation ? PDC_ENOMEM : PDC_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(s, e_, what); \
+    } while (0)
+
+static pdc::EngineCfg engine_cfg(const pdc_config& c) {
+    pdc::EngineCfg e;
+    e.max_iter = c.max_iter;
+    e.tol = c.tol;
+    e.mu = c.mu;
+    e.restitution = c.restitution;
+    e.spring_based = c.spring_based;
+    e.compliance_coef = 0;
+    e.spring_k = c.spring_k;
+    e.spring_damp = c.spring_damp;
+    e.direct_threshold = c.direct_threshold;
+    e.dense_max = c.dense_max_bodies;
+    e.rtol_direct = c.pcg_rtol_direct;
+    e.max_direct = c.pcg_max_direct;
+    e.rtol_iter = c.pcg_rtol_iter;
+    e.max_cg = c.pcg_max_iter;
+    return e;
+}
+
+// Workspace layout for a batch with totals (ns, nb, nc).
+static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs* P, bool host_inputs, int grid,
+                    int dense_max) {
+    A.reset();
+    auto D = [&](size_t n) { return A.take<double>(n); };
+    auto I = [&](size_t n) { return A.take<int>(n); };
+    if (host_inputs) {
+        P->body_off = I(ns + 1);
+        P->contact_off = I(ns + 1);
+        P->dt = D(ns);
+        P->grav = D(3 * ns);
+        P->order = I(ns);
+        P->vel = D(3 * nb);
+        P->ang = D(3 * nb);
+        P->mass = D(nb);
+        P->inertia = D(6 * nb);
+        P->inv_inertia = D(6 * nb);
+        P->is_static = A.take<uint8_t>(nb);
+        P->cbody = I(2 * nc);
+        P->frame = D(9 * nc);
+        P->arm = D(6 * nc);
+        P->depth = D(nc);
+        P->cmu = D(nc);
+        P->dvel = D(3 * nb);
+        P->dang = D(3 * nb);
+        P->lforce = D(3 * nc);
+        P->stats = A.take<pdc_stats>(ns);
+    }
+    P->inc_start = I(nb);
+    P->inc_cnt = I(nb);
+    P->inc_cur = I(nb);
+    P->local = A.take<uint8_t>(nb);
+    P->u = D(6 * nb);
+    P->uold = D(6 * nb);
+    P->du = D(6 * nb);
+    P->r = D(6 * nb);
+    P->z = D(6 * nb);
+    P->p = D(6 * nb);
+    P->rhs = D(6 * nb);
+    P->ru = D(6 * nb);
+    P->pinv = D(21 * nb);
+    P->inc = I(2 * nc);
+    P->f = D(3 * nc);
+    P->lam = D(2 * nc);
+    P->fT = D(3 * nc);
+    P->lT = D(2 * nc);
+    P->df = D(3 * nc);
+    P->dl = D(2 * nc);
+    P->rf = D(3 * nc);
+    P->rl = D(2 * nc);
+    P->kn = D(nc);
+    P->cv = D(2 * nc);
+    P->gr = D(2 * nc);
+    P->hs = D(3 * nc);
+    P->invC = D(2 * nc);
+    P->knInv = D(nc);
+    P->ktInv = D(3 * nc);
+    P->sf = D(3 * nc);
+    P->X = D(3 * nc);
+    P->W = D(6 * nc);
+    P->didx = I(nb);
+    P->dbody = I(nb);
+    if (dense_max > 0) {
+        const long long NM = 6LL * dense_max;
+        P->dense_stride = NM * NM + 3 * NM;
+        P->dense = D((size_t)grid * P->dense_stride);
+    } else {
+        P->dense = nullptr;
+        P->dense_stride = 0;
+    }
+    return A.off + 256;
+}
+
+static int grid_for(const pdc_solver* s, int ns) { return std::max(1, std::min(ns, s->num_sms * s->blocks_per_sm)); }
+
+static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::BatchPtrs* P, bool host_inputs) {
+    const int grid = grid_for(s, ns);
+    const int dmax = s->cfg.dense_max_bodies;
+    Arena probe;
+    probe.base = nullptr;
+    size_t need = carve(probe, ns, nb, nc, P, host_inputs, grid, dmax);
+    if (need > s->arena.cap) {
+        const size_t cap = std::max(need, s->arena.cap * 2);
+        if (s->arena.base) cudaFree(s->arena.base);
+        s->arena.base = nullptr;
+        s->arena.cap = 0;
+        cudaError_t e = cudaMalloc(&s->arena.base, cap);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_fail(s, e, "cudaMalloc(workspace)");
+        }
+        s->arena.cap = cap;
+    }
+    carve(s->arena, ns, nb, nc, P, host_inputs, grid, dmax);
+    return PDC_OK;
+}
+
+extern "C" void pdc_config_default(pdc_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->abi_version = PDC_ABI_VERSION;
+    c->max_iter = 100;   // PrimalDualForceSolver.cpp:652
+    c->tol = 1e-6;       // :651
+    c->force_model = PDC_FORCE_NON_SMOOTH_CONTACT;
+    c->spring_based = 0;
+    c->mu = 0.5;         // NonSmoothContactForce.cpp:332
+    c->restitution = 0;  // :329
+    c->spring_k = 1e6;   // :324
+    c->spring_damp = 0.01;
+    c->precision = PDC_PRECISION_FP64;
+    c->direct_threshold = 2000;  // :385
+    c->dense_max_bodies = 64;
+    c->pcg_rtol_direct = 1e-13;
+    c->pcg_max_direct = 4000;
+    c->pcg_rtol_iter = 1e-8;
+    c->pcg_max_iter = 1000;  // :381
+    c->mixed_inner_rtol = 1e-3;
+    c->warm_start = 0;
+    c->device = 0;
+}
+
+static int validate_config(pdc_solver* s, const pdc_config* c) {
+    if (!c) return fail(s, PDC_EINVAL, "null config");
+    if (c->abi_version != PDC_ABI_VERSION) return fail(s, PDC_EINVAL, "ABI version mismatch");
+    if (c->max_iter < 0 || !(c->tol >= 0)) return fail(s, PDC_EINVAL, "bad iterations/tolerance");
+    if (c->force_model != PDC_FORCE_NON_SMOOTH_CONTACT)
+        return fail(s, PDC_EINVAL, "non-smooth force model not supported by the GPU path");
+    if (c->precision != PDC_PRECISION_FP64 && c->precision != PDC_PRECISION_MIXED)
+        return fail(s, PDC_EINVAL, "unknown precision");
+    if (c->pcg_max_direct <= 0 || c->pcg_max_iter <= 0) return fail(s, PDC_EINVAL, "bad PCG caps");
+    if (c->dense_max_bodies < 0 || c->dense_max_bodies > 256) return fail(s, PDC_EINVAL, "dense_max_bodies out of [0, 256]");
+    return PDC_OK;
+}
+
+extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
+    if (!out) return fail(nullptr, PDC_EINVAL, "null output handle");
+    *out = nullptr;
+    int rc = validate_config(nullptr, cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, PDC_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, PDC_EINVAL, "bad device ordinal");
+    pdc_solver* s = new pdc_solver();
+    s->cfg = *cfg;
+    s->device = cfg->device;
+    e = cudaSetDevice(s->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel, 256, 0);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_timers, 4 * sizeof(unsigned long long) + 16);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_counter, 16);
+    if (e == cudaSuccess) e = cudaMemset(s->d_timers, 0, 4 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_create_error = std::string("CUDA set-up failed: ") + cudaGetErrorString(e);
+        pdc_destroy(s);
+        return PDC_ECUDA;
+    }
+    if (s->blocks_per_sm < 1) s->blocks_per_sm = 1;
+    *out = s;
+    return PDC_OK;
+}
+
+extern "C" void pdc_destroy(pdc_solver* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->arena.base) cudaFree(s->arena.base);
+    if (s->d_timers) cudaFree(s->d_timers);
+    if (s->d_counter) cudaFree(s->d_counter);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+extern "C" int pdc_reset(pdc_solver* s) {
+    if (!s) return PDC_EINVAL;
+    cudaSetDevice(s->device);
+    CK(cudaStreamSynchronize(s->stream), "sync");
+    CK(cudaMemset(s->d_timers, 0, 4 * sizeof(unsigned long long)), "memset timers");
+    s->t_total = s->t_build = s->t_solve = s->t_ls = 0;
+    s->newton_total = 0;
+    s->solves = 0;
+    return PDC_OK;
+}
+
+static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st) {
+    pdc::BatchPtrs P = P0;
+    P.work_counter = s->d_counter;
+    P.timers = s->d_timers;
+    CK(cudaMemsetAsync(s->d_counter, 0, sizeof(int), st), "memset counter");
+    if (P.n_scenes == 0) return PDC_OK;
+    const int grid = grid_for(s, P.n_scenes);
+    pdc::EngineCfg C = engine_cfg(s->cfg);
+    pdc::solve_scenes_kernel<<<grid, 256, 0, st>>>(P, C);
+    CK(cudaGetLastError(), "launch solve_scenes_kernel");
+    return PDC_OK;
+}
+
+// Host-array validation shared by pdc_solve and pdc_batch_solve.
+static int validate_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_soa* b,
+                         const pdc_contacts_soa* c) {
+    if (!b || !c || !batch) return fail(s, PDC_EINVAL, "null argument");
+    if (b->n < 0 || c->n < 0) return fail(s, PDC_EINVAL, "negative size");
+    if (b->n > 0 && (!b->vel || !b->ang_vel || !b->mass || !b->inertia || !b->inv_inertia))
+        return fail(s, PDC_EINVAL, "null body array");
+    if (c->n > 0 && (!c->body || !c->frame || !c->arm)) return fail(s, PDC_EINVAL, "null contact array");
+    const int ns = batch->n_scenes;
+    if (ns < 0) return fail(s, PDC_EINVAL, "negative scene count");
+    if (ns > 0 && (!batch->body_offsets || !batch->contact_offsets || !batch->dt || !batch->gravity))
+        return fail(s, PDC_EINVAL, "null batch array");
+    if (ns > 0 && (batch->body_offsets[0] != 0 || batch->contact_offsets[0] != 0 ||
+                   batch->body_offsets[ns] != b->n || batch->contact_offsets[ns] != c->n))
+        return fail(s, PDC_EINVAL, "batch offsets do not cover the arrays");
+    for (int k = 0; k < ns; ++k) {
+        const int nb = batch->body_offsets[k + 1] - batch->body_offsets[k];
+        const int c0 = batch->contact_offsets[k], c1 = batch->contact_offsets[k + 1];
+        if (nb < 0 || c1 < c0) return fail(s, PDC_EINVAL, "non-monotone batch offsets");
+        for (int q = c0; q < c1; ++q)
+            for (int j = 0; j < 2; ++j) {
+                const int id = c->body[2 * q + j];
+                if (id < 0 || id >= nb) return fail(s, PDC_EINVAL, "contact body id out of range");
+            }
+        if (!(batch->dt[k] > 0)) return fail(s, PDC_EINVAL, "time step must be positive");
+    }
+    return PDC_OK;
+}
+
+static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_soa* b, const pdc_contacts_soa* c,
+                      double* dvel, double* dang, double* lforce, pdc_stats* stats) {
+    int rc = validate_host(s, batch, b, c);
+    if (rc) return rc;
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    const int ns = batch->n_scenes;
+    const long long nb = b->n, nc = c->n;
+    pdc::BatchPtrs P;
+    std::memset(&P, 0, sizeof(P));
+    rc = ensure_arena(s, ns, std::max(nb, 1LL), std::max(nc, 1LL), &P, true);
+    if (rc) return rc;
+    P.n_scenes = ns;
+    cudaStream_t st = s->stream;
+    // largest scenes first for load balance across CTAs
+    std::vector<int> order(ns);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return (batch->contact_offsets[x + 1] - batch->contact_offsets[x]) >
+               (batch->contact_offsets[y + 1] - batch->contact_offsets[y]);
+    });
+    std::vector<double> mu_fill;
+    auto H2D = [&](const void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    CK(H2D(P.body_off, batch->body_offsets, (ns + 1) * sizeof(int)), "H2D");
+    CK(H2D(P.contact_off, batch->contact_offsets, (ns + 1) * sizeof(int)), "H2D");
+    CK(H2D(P.dt, batch->dt, ns * sizeof(double)), "H2D");
+    CK(H2D(P.grav, batch->gravity, 3 * ns * sizeof(double)), "H2D");
+    CK(H2D(P.order, order.data(), ns * sizeof(int)), "H2D");
+    if (nb) {
+        CK(H2D(P.vel, b->vel, 3 * nb * sizeof(double)), "H2D");
+        CK(H2D(P.ang, b->ang_vel, 3 * nb * sizeof(double)), "H2D");
+        CK(H2D(P.mass, b->mass, nb * sizeof(double)), "H2D");
+        CK(H2D(P.inertia, b->inertia, 6 * nb * sizeof(double)), "H2D");
+        CK(H2D(P.inv_inertia, b->inv_inertia, 6 * nb * sizeof(double)), "H2D");
+        if (b->is_static) CK(H2D(P.is_static, b->is_static, nb), "H2D");
+        else CK(cudaMemsetAsync(const_cast<uint8_t*>(P.is_static), 0, nb, st), "memset");
+    }
+    if (nc) {
+        CK(H2D(P.cbody, c->body, 2 * nc * sizeof(int)), "H2D");
+        CK(H2D(P.frame, c->frame, 9 * nc * sizeof(double)), "H2D");
+        CK(H2D(P.arm, c->arm, 6 * nc * sizeof(double)), "H2D");
+        if (c->depth) CK(H2D(P.depth, c->depth, nc * sizeof(double)), "H2D");
+        else CK(cudaMemsetAsync(const_cast<double*>(P.depth), 0, nc * sizeof(double), st), "memset");
+        if (c->mu) CK(H2D(P.cmu, c->mu, nc * sizeof(double)), "H2D");
+        else P.cmu = nullptr;
+    } else {
+        P.cmu = nullptr;
+    }
+    rc = launch(s, P, st);
+    if (rc) return rc;
+    if (nb) {
+        CK(cudaMemcpyAsync(dvel, P.dvel, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        CK(cudaMemcpyAsync(dang, P.dang, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    }
+    if (nc) CK(cudaMemcpyAsync(lforce, P.lforce, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    std::vector<pdc_stats> hst(ns);
+    if (ns) CK(cudaMemcpyAsync(hst.data(), P.stats, ns * sizeof(pdc_stats), cudaMemcpyDeviceToHost, st), "D2H");
+    CK(cudaStreamSynchronize(st), "solve");
+    for (int k = 0; k < ns; ++k) {
+        s->newton_total += hst[k].newton_iters;
+        if (stats) stats[k] = hst[k];
+    }
+    s->solves += ns;
+    return PDC_OK;
+}
+
+extern "C" int pdc_solve(pdc_solver* s, double dt, const double gravity[3], const pdc_bodies_soa* bodies,
+                         const pdc_contacts_soa* contacts, pdc_result* out) {
+    if (!s) return PDC_EINVAL;
+    if (!gravity || !out || !bodies || !contacts) return fail(s, PDC_EINVAL, "null argument");
+    int off_b[2] = {0, bodies->n}, off_c[2] = {0, contacts->n};
+    pdc_batch bt;
+    bt.n_scenes = 1;
+    bt.body_offsets = off_b;
+    bt.contact_offsets = off_c;
+    bt.dt = &dt;
+    bt.gravity = gravity;
+    std::memset(&out->stats, 0, sizeof(out->stats));
+    return batch_host(s, &bt, bodies, contacts, out->dvel, out->dang_vel, out->local_force, &out->stats);
+}
+
+extern "C" int pdc_batch_solve(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_soa* bodies,
+                               const pdc_contacts_soa* contacts, double* dvel, double* dang_vel,
+                               double* local_force, pdc_stats* stats) {
+    if (!s) return PDC_EINVAL;
+    return batch_host(s, batch, bodies, contacts, dvel, dang_vel, local_force, stats);
+}
+
+extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_soa* b,
+                                     const pdc_contacts_soa* c, double* dvel, double* dang_vel,
+                                     double* local_force, pdc_stats* stats, void* stream) {
+    if (!s) return PDC_EINVAL;
+    if (!batch || !b || !c || !dvel || !dang_vel || !local_force) return fail(s, PDC_EINVAL, "null argument");
+    if (batch->n_scenes < 0 || b->n < 0 || c->n < 0) return fail(s, PDC_EINVAL, "negative size");
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    pdc::BatchPtrs P;
+    std::memset(&P, 0, sizeof(P));
+    int rc = ensure_arena(s, batch->n_scenes, std::max(b->n, 1), std::max(c->n, 1), &P, false);
+    if (rc) return rc;
+    P.n_scenes = batch->n_scenes;
+    P.body_off = batch->body_offsets;
+    P.contact_off = batch->contact_offsets;
+    P.dt = batch->dt;
+    P.grav = batch->gravity;
+    P.order = nullptr;
+    P.vel = b->vel;
+    P.ang = b->ang_vel;
+    P.mass = b->mass;
+    P.inertia = b->inertia;
+    P.inv_inertia = b->inv_inertia;
+    P.is_static = b->is_static;
+    P.cbody = c->body;
+    P.frame = c->frame;
+    P.arm = c->arm;
+    P.depth = c->depth;
+    P.cmu = c->mu;
+    P.dvel = dvel;
+    P.dang = dang_vel;
+    P.lforce = local_force;
+    P.stats = stats;
+    if (!P.is_static || !P.depth) return fail(s, PDC_EINVAL, "device path needs is_static and depth arrays");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    rc = launch(s, P, st);
+    if (rc) return rc;
+    s->solves += batch->n_scenes;
+    return PDC_OK;
+}
+
+extern "C" int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3], const pdc_bodies_soa* bodies,
+                               const pdc_contacts_soa* contacts, pdc_result* out, void* stream) {
+    (void)dt;
+    (void)gravity;
+    (void)bodies;
+    (void)contacts;
+    (void)out;
+    (void)stream;
+    return fail(s, PDC_EINVAL, "pdc_solve_async: use pdc_batch_solve_async with one scene");
+}
+
+extern "C" int pdc_sync(pdc_solver* s, int32_t timeout_ms) {
+    if (!s) return PDC_EINVAL;
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    // bounded wait: poll the stream, never block forever
+    const long long limit_us = (long long)(timeout_ms > 0 ? timeout_ms : 60000) * 1000;
+    long long waited = 0;
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(s->stream);
+        if (e == cudaSuccess) return PDC_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(s, e, "stream");
+        if (waited >= limit_us) return fail(s, PDC_ETIMEOUT, "pdc_sync timed out");
+        struct timespec ts = {0, 50000};
+        nanosleep(&ts, nullptr);
+        waited += 50;
+    }
+}
+
+extern "C" int pdc_timings(pdc_solver* s, double out[6]) {
+    if (!s || !out) return PDC_EINVAL;
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(s->stream), "sync");
+    unsigned long long t[4];
+    CK(cudaMemcpy(t, s->d_timers, sizeof(t), cudaMemcpyDeviceToHost), "D2H timers");
+    for (int k = 0; k < 4; ++k) out[k] = t[k] * 1e-9;
+    out[4] = (double)s->newton_total;
+    out[5] = (double)s->solves;
+    return PDC_OK;
+}
+
+extern "C" const char* pdc_last_error(const pdc_solver* s) {
+    return s ? s->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" const char* pdc_version(void) { return "pdc-b200 0.1 (sm_100a)"; }

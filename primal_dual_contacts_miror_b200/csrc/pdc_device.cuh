@@ -1,0 +1,172 @@
+// Device-side building blocks of the B200 contact solver: small 3-vector math,
+// the friction-cone functions, and deterministic block reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pdc {
+
+// ------------------------------------------------------------ small math
+struct d3 { double x, y, z; };
+__device__ __forceinline__ d3 mk3(double a, double b, double c) { return d3{a, b, c}; }
+__device__ __forceinline__ d3 add3(d3 a, d3 b) { return d3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ d3 sub3(d3 a, d3 b) { return d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ d3 scl3(double s, d3 a) { return d3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double dot3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross3(d3 a, d3 b) {
+    return d3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ d3 ld3(const double* p) { return d3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void st3(double* p, d3 v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+
+// Contact frame R (row-major 3x3, columns n, t1, t2).
+struct Frame { double m[9]; };
+__device__ __forceinline__ Frame ld_frame(const double* __restrict__ p) {
+    Frame f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f.m[i] = __ldg(p + i);
+    return f;
+}
+// R^T v  (world -> contact frame)
+__device__ __forceinline__ d3 to_frame(const Frame& R, d3 v) {
+    return d3{R.m[0] * v.x + R.m[3] * v.y + R.m[6] * v.z,
+              R.m[1] * v.x + R.m[4] * v.y + R.m[7] * v.z,
+              R.m[2] * v.x + R.m[5] * v.y + R.m[8] * v.z};
+}
+// R f  (contact frame -> world)
+__device__ __forceinline__ d3 from_frame(const Frame& R, d3 f) {
+    return d3{R.m[0] * f.x + R.m[1] * f.y + R.m[2] * f.z,
+              R.m[3] * f.x + R.m[4] * f.y + R.m[5] * f.z,
+              R.m[6] * f.x + R.m[7] * f.y + R.m[8] * f.z};
+}
+
+// ------------------------------------------------ friction cone (a11)
+// c(f) = sqrt(ft^2 + p) - mu fn - sqrt(p) - shift, p = 1e-16, shift = 1e-8
+// (LorentzCircleConstraint.cpp:5-13, .h:18-19).
+#define PDC_PERT 1e-16
+#define PDC_SQRT_PERT 1e-8
+#define PDC_SHIFT 1e-8
+__device__ __forceinline__ double cone_c(double fn, double f1, double f2, double mu) {
+    double r = f1 * f1 + f2 * f2 + PDC_PERT;
+    return sqrt(r) - mu * fn - PDC_SQRT_PERT - PDC_SHIFT;
+}
+__device__ __forceinline__ void cone_grad(double f1, double f2, double& g0, double& g1) {
+    double r = sqrt(f1 * f1 + f2 * f2 + PDC_PERT);
+    g0 = f1 / r;
+    g1 = f2 / r;
+}
+// Hessian (zz^T + p'I) r2^-3/2 with z = (f2, -f1), p' = 1e-6 (:23-35); packed (h00, h01, h11).
+__device__ __forceinline__ void cone_hess(double f1, double f2, double& h00, double& h01, double& h11) {
+    const double p = 1e-6;
+    double r2 = f1 * f1 + f2 * f2 + p;
+    double r3 = pow(r2, -1.5);
+    h00 = (f2 * f2 + p) * r3;
+    h01 = (f2 * -f1) * r3;
+    h11 = (f1 * f1 + p) * r3;
+}
+__device__ __forceinline__ double cone_radius(double fn, double mu) {
+    double k = mu * fn + PDC_SQRT_PERT + PDC_SHIFT;
+    return sqrt(k * k - PDC_PERT);
+}
+
+// ------------------------------------------- deterministic block reductions
+// Every thread passes its partial sums; every thread receives the identical
+// total (fixed tree: warp shuffle-down to lane 0, per-warp slots, then the same
+// tree over the slots in every warp).  `buf` alternates between two halves so a
+// single __syncthreads per reduction suffices.
+template <int N>
+struct BlockReducer {
+    double* slots;  // [2][N][32] in shared memory
+    int parity;
+    __device__ void init(double* s) { slots = s; parity = 0; }
+    __device__ __forceinline__ void sum(double (&v)[N]) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        double* b = slots + parity * N * 32;
+        parity ^= 1;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) b[i * 32 + warp] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = (lane < nw) ? b[i * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            v[i] = __shfl_sync(0xffffffffu, x, 0);
+        }
+    }
+    __device__ __forceinline__ void max(double (&v)[N]) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        double* b = slots + parity * N * 32;
+        parity ^= 1;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_down_sync(0xffffffffu, x, o));
+            if (lane == 0) b[i * 32 + warp] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = (lane < nw) ? b[i * 32 + lane] : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_down_sync(0xffffffffu, x, o));
+            v[i] = __shfl_sync(0xffffffffu, x, 0);
+        }
+    }
+};
+
+// 6x6 symmetric positive definite inverse via Cholesky; input/output packed
+// lower triangle, row-major (21 values: (0,0),(1,0),(1,1),(2,0),...).
+__device__ __forceinline__ int pk(int r, int c) { return (r >= c) ? (r * (r + 1) / 2 + c) : (c * (c + 1) / 2 + r); }
+__device__ inline bool spd6_inverse(const double* A, double* Ainv) {
+    double L[21];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        double d = A[pk(j, j)];
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= L[pk(j, k)] * L[pk(j, k)];
+        if (!(d > 0.0)) return false;
+        double ljj = sqrt(d);
+        L[pk(j, j)] = ljj;
+#pragma unroll
+        for (int i = j + 1; i < 6; ++i) {
+            double s = A[pk(i, j)];
+#pragma unroll
+            for (int k = 0; k < j; ++k) s -= L[pk(i, k)] * L[pk(j, k)];
+            L[pk(i, j)] = s / ljj;
+        }
+    }
+    // inverse of L (lower), then Ainv = L^-T L^-1
+    double Li[21];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        Li[pk(j, j)] = 1.0 / L[pk(j, j)];
+#pragma unroll
+        for (int i = j + 1; i < 6; ++i) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = j; k < i; ++k) s -= L[pk(i, k)] * Li[pk(k, j)];
+            Li[pk(i, j)] = s / L[pk(i, i)];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = r; k < 6; ++k) s += Li[pk(k, r)] * Li[pk(k, c)];
+            Ainv[pk(r, c)] = s;
+        }
+    return true;
+}
+
+}  // namespace pdc

@@ -1,0 +1,1194 @@
+// The primal-dual interior-point Newton solve of one contact scene, executed by
+// one thread block (CTA) with __syncthreads between phases.  A batched launch
+// hands scenes to CTAs from an atomic work counter, so thousands of small,
+// ragged scenes run concurrently on the 148 SMs of a B200, each scene's
+// working set staying L1/L2 resident while its CTA iterates.
+//
+// Algorithm: the reference's PrimalDualForceSolver::fillForcesIntl
+// (src/Solver/PrimalDual/PrimalDualForceSolver.cpp:167-511) with
+// NonSmoothContactForce (src/Solver/PrimalDual/NonSmoothForces/NonSmoothContactForce.cpp:8-319).
+// Differences in mechanism, not in the solution:
+//  * the 6N_b x 6N_b Newton system is never assembled; its product with a
+//    vector is applied matrix-free per contact (W = R K^-1 R^T, 6 doubles) and
+//    gathered per body;
+//  * the LDL^T / AMGCL solve (:385-427) is a block-Jacobi preconditioned CG,
+//    converged to cfg.rtol_direct (direct branch) or cfg.rtol_iter with the
+//    reference's AMGCL cap and Hu rule (iterative branch, >= 2000 local bodies);
+//  * the contact->body scatter, which the reference does with omp atomics
+//    (NonSmoothContactForce.cpp:144,228,243), is a gather over per-body
+//    incidence lists sorted by contact index, so results are bitwise
+//    reproducible run to run.
+#pragma once
+#include "pdc_device.cuh"
+#include "../../include/pdc.h"
+
+namespace pdc {
+
+struct EngineCfg {
+    int max_iter;
+    double tol;
+    double mu;
+    double restitution;
+    int spring_based;
+    double compliance_coef;  // m_compliance numerator inputs
+    double spring_k, spring_damp;
+    int direct_threshold;
+    int dense_max;  // direct branch: dense Cholesky up to this many active bodies
+    double rtol_direct;
+    int max_direct;
+    double rtol_iter;
+    int max_cg;
+};
+
+struct BatchPtrs {
+    int n_scenes;
+    const int* __restrict__ body_off;
+    const int* __restrict__ contact_off;
+    const double* __restrict__ dt;
+    const double* __restrict__ grav;
+    const int* __restrict__ order;  // optional scene order (may be null)
+    // bodies (inputs)
+    const double* __restrict__ vel;
+    const double* __restrict__ ang;
+    const double* __restrict__ mass;
+    const double* __restrict__ inertia;
+    const double* __restrict__ inv_inertia;
+    const uint8_t* __restrict__ is_static;
+    // contacts (inputs)
+    const int* __restrict__ cbody;
+    const double* __restrict__ frame;
+    const double* __restrict__ arm;
+    const double* __restrict__ depth;
+    const double* __restrict__ cmu;
+    // outputs
+    double* dvel;
+    double* dang;
+    double* lforce;
+    pdc_stats* stats;
+    // per-body workspace
+    int* inc_start;
+    int* inc_cnt;
+    int* inc_cur;
+    uint8_t* local;
+    double* u;     // 6
+    double* uold;  // 6
+    double* du;    // 6
+    double* r;     // 6
+    double* z;     // 6
+    double* p;     // 6
+    double* rhs;   // 6
+    double* ru;    // 6
+    double* pinv;  // 21
+    // per-contact workspace
+    int* inc;       // 2 per contact
+    double* f;      // 3
+    double* lam;    // 2
+    double* fT;     // 3
+    double* lT;     // 2
+    double* df;     // 3
+    double* dl;     // 2
+    double* rf;     // 3
+    double* rl;     // 2
+    double* kn;     // 1 (m_nonSmoothK normal slot)
+    double* cv;     // 2 constraint values
+    double* gr;     // 2 gradients
+    double* hs;     // 3 hessian (packed)
+    double* invC;   // 2
+    double* knInv;  // 1
+    double* ktInv;  // 3 (packed symmetric inverse of K_t)
+    double* sf;     // 3
+    double* X;      // 3 world vector gathered by bodies
+    double* W;      // 6 R K^-1 R^T packed (xx,yy,zz,xy,xz,yz)
+    int* didx;   // dense row-block of each active body
+    int* dbody;  // body of each dense row-block (scene-relative slots)
+    // per-CTA dense scratch: (6 dense_max)^2 matrix + 3 vectors of 6 dense_max
+    double* dense;
+    long long dense_stride;
+    int* work_counter;
+    unsigned long long* timers;  // [4] ns: total, build, solve, line search
+};
+
+#define PDC_STATUS_BAD_INPUT 16
+
+// W = R diag(kn, Kt^-1) R^T (packed symmetric)
+__device__ __forceinline__ void frame_sandwich(const Frame& R, double kni, double t00, double t01, double t11,
+                                               double* W) {
+    // columns of R: n = (m0,m3,m6), t1 = (m1,m4,m7), t2 = (m2,m5,m8)
+    double K[3][3] = {{kni, 0, 0}, {0, t00, t01}, {0, t01, t11}};
+    double RK[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) RK[i][j] = R.m[i * 3 + 0] * K[0][j] + R.m[i * 3 + 1] * K[1][j] + R.m[i * 3 + 2] * K[2][j];
+    auto e = [&](int i, int j) { return RK[i][0] * R.m[j * 3 + 0] + RK[i][1] * R.m[j * 3 + 1] + RK[i][2] * R.m[j * 3 + 2]; };
+    W[0] = e(0, 0);
+    W[1] = e(1, 1);
+    W[2] = e(2, 2);
+    W[3] = e(0, 1);
+    W[4] = e(0, 2);
+    W[5] = e(1, 2);
+}
+__device__ __forceinline__ d3 sym_mul(const double* W, d3 v) {
+    return d3{W[0] * v.x + W[3] * v.y + W[4] * v.z, W[3] * v.x + W[1] * v.y + W[5] * v.z,
+              W[4] * v.x + W[5] * v.y + W[2] * v.z};
+}
+
+// Velocity of the contact point on body j: v + w x c  (zero for static / non-active)
+__device__ __forceinline__ d3 point_vel(const double* u6, d3 c) {
+    d3 v = ld3(u6), w = ld3(u6 + 3);
+    return add3(v, cross3(w, c));
+}
+
+class SceneSolver {
+   public:
+    const BatchPtrs& B;
+    const EngineCfg& C;
+    BlockReducer<8>& red;
+    int s, b0, nb, c0, nc, tid, nt;
+    double dt, g[3];
+    double cm, cs;  // charMass, charSpeed
+    double compliance, reduction, spring_term;
+    int n_local, n_active;
+    bool dense_mode;
+    int status;
+    unsigned long long t_build, t_solve, t_ls, t_mark;
+
+    __device__ SceneSolver(const BatchPtrs& b, const EngineCfg& c, BlockReducer<8>& r, int scene)
+        : B(b), C(c), red(r), s(scene) {
+        b0 = B.body_off[s];
+        nb = B.body_off[s + 1] - b0;
+        c0 = B.contact_off[s];
+        nc = B.contact_off[s + 1] - c0;
+        tid = threadIdx.x;
+        nt = blockDim.x;
+        dt = B.dt[s];
+        g[0] = B.grav[3 * s];
+        g[1] = B.grav[3 * s + 1];
+        g[2] = B.grav[3 * s + 2];
+        status = 0;
+        t_build = t_solve = t_ls = 0;
+    }
+
+    __device__ __forceinline__ unsigned long long now() {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+    __device__ __forceinline__ bool active(int gb) const { return B.local[gb] && !B.is_static[gb]; }
+    __device__ __forceinline__ double cmu(int gc) const { return B.cmu ? B.cmu[gc] : C.mu; }
+
+    // Gather sum over the incidences of body gb of sigma * [X; c x X]
+    __device__ __forceinline__ void gather(int gb, double out[6]) const {
+        const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+        for (int k = 0; k < n; ++k) {
+            const int e = B.inc[st + k];
+            const int gc = e >> 1, side = e & 1;
+            d3 x = ld3(B.X + 3 * gc);
+            d3 arm = ld3(B.arm + 6 * gc + 3 * side);
+            if (!side) x = scl3(-1.0, x);
+            d3 t = cross3(arm, x);
+            a0 += x.x; a1 += x.y; a2 += x.z;
+            a3 += t.x; a4 += t.y; a5 += t.z;
+        }
+        out[0] = a0; out[1] = a1; out[2] = a2; out[3] = a3; out[4] = a4; out[5] = a5;
+    }
+    // (M / charMass) v  for an active body
+    __device__ __forceinline__ void mass_mul(int gb, const double* v, double* y) const {
+        const double m = B.mass[gb] / cm;
+        const double* I = B.inertia + 6 * gb;
+        double Ixx = I[0] / cm, Iyy = I[1] / cm, Izz = I[2] / cm, Ixy = I[3] / cm, Ixz = I[4] / cm, Iyz = I[5] / cm;
+        y[0] = m * v[0];
+        y[1] = m * v[1];
+        y[2] = m * v[2];
+        y[3] = Ixx * v[3] + Ixy * v[4] + Ixz * v[5];
+        y[4] = Ixy * v[3] + Iyy * v[4] + Iyz * v[5];
+        y[5] = Ixz * v[3] + Iyz * v[4] + Izz * v[5];
+    }
+
+    // Block-wide exclusive scan over the scene's bodies: put(b, carry0 + prefix).
+    template <typename Get, typename Put>
+    __device__ void block_scan(int carry0, Get get, Put put) {
+        __shared__ int s_carry;
+        __shared__ int s_warp[32];
+        if (tid == 0) s_carry = carry0;
+        __syncthreads();
+        for (int base = 0; base < nb; base += nt) {
+            const int b = base + tid;
+            const int val = (b < nb) ? get(b) : 0;
+            int x = val;
+            const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_warp[warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                int w = (lane < (nt >> 5)) ? s_warp[lane] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                s_warp[lane] = w;
+            }
+            __syncthreads();
+            const int excl = x - val + (warp ? s_warp[warp - 1] : 0) + s_carry;
+            if (b < nb) put(b, excl);
+            __syncthreads();
+            if (tid == nt - 1) s_carry = excl + val;
+            __syncthreads();
+        }
+    }
+
+    // ------------------------------------------------------------ set-up
+    // Returns false if the scene has no contacts (outputs already written).
+    __device__ bool setup() {
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            B.dvel[3 * gb] = g[0] * dt;  // fillForces :85-88
+            B.dvel[3 * gb + 1] = g[1] * dt;
+            B.dvel[3 * gb + 2] = g[2] * dt;
+            B.dang[3 * gb] = 0;
+            B.dang[3 * gb + 1] = 0;
+            B.dang[3 * gb + 2] = 0;
+            B.inc_cnt[gb] = 0;
+            B.inc_cur[gb] = 0;
+            B.local[gb] = 0;
+        }
+        if (nc == 0) return false;
+        __syncthreads();
+        // count incidences, mark local bodies (renumbering :95-118)
+        int bad = 0;
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            for (int j = 0; j < 2; ++j) {
+                const int b = B.cbody[2 * gc + j];
+                if (b < 0 || b >= nb) { bad = 1; continue; }
+                B.local[b0 + b] = 1;
+                if (!B.is_static[b0 + b]) atomicAdd(&B.inc_cnt[b0 + b], 1);
+            }
+        }
+        double v[8] = {(double)bad, 0, 0, 0, 0, 0, 0, 0};
+        red.max(v);
+        if (v[0] > 0) { status |= PDC_STATUS_BAD_INPUT; return false; }
+        // exclusive scan of counts -> absolute start in inc[]
+        block_scan(2 * c0, [&](int b) { return B.inc_cnt[b0 + b]; },
+                   [&](int b, int excl) { B.inc_start[b0 + b] = excl; });
+        // fill incidence lists (slot order arbitrary, sorted below)
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            for (int j = 0; j < 2; ++j) {
+                const int gb = b0 + B.cbody[2 * gc + j];
+                if (B.is_static[gb]) continue;
+                const int slot = atomicAdd(&B.inc_cur[gb], 1);
+                B.inc[B.inc_start[gb] + slot] = (gc << 1) | j;
+            }
+        }
+        // per-contact speeds for nonDimensionalParams (:38-63): velExt = v (+ g dt if active)
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            const Frame R = ld_frame(B.frame + 9 * gc);
+            d3 half[2];
+            bool hasStatic = false;
+            for (int j = 0; j < 2; ++j) {
+                const int gb = b0 + B.cbody[2 * gc + j];
+                double ve[6];
+                for (int r = 0; r < 3; ++r) {
+                    ve[r] = B.vel[3 * gb + r];
+                    ve[3 + r] = B.ang[3 * gb + r];
+                }
+                if (!B.is_static[gb]) {
+                    for (int r = 0; r < 3; ++r) ve[r] += g[r] * dt;
+                } else {
+                    hasStatic = true;
+                }
+                // toLocal(j, velExt) = -T_j^T velExt: j=0 -> -R^T(v + w x c0); j=1 -> +R^T(v + w x c1)
+                d3 pv = point_vel(ve, ld3(B.arm + 6 * gc + 3 * j));
+                d3 h = to_frame(R, pv);
+                half[j] = j ? h : scl3(-1.0, h);
+            }
+            d3 rel = add3(half[0], half[1]);
+            const double nrel = sqrt(dot3(rel, rel));
+            for (int j = 0; j < 2; ++j) {
+                double sp = sqrt(dot3(half[j], half[j]));
+                if (hasStatic) sp = dmax(sp, nrel);
+                B.X[3 * gc + j] = sp;
+            }
+        }
+        __syncthreads();
+        // sort incidence lists, per-body speed, mass sums
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // n_local, n_active, traceSum, m*speed, m
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            if (!B.local[gb]) continue;
+            acc[0] += 1;
+            if (B.is_static[gb]) continue;
+            const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+            for (int i = 1; i < n; ++i) {  // insertion sort by (contact, side)
+                const int key = B.inc[st + i];
+                int j = i - 1;
+                while (j >= 0 && B.inc[st + j] > key) {
+                    B.inc[st + j + 1] = B.inc[st + j];
+                    --j;
+                }
+                B.inc[st + j + 1] = key;
+            }
+            double spd = 0;
+            for (int k = 0; k < n; ++k) {
+                const int e = B.inc[st + k];
+                spd = dmax(spd, B.X[3 * (e >> 1) + (e & 1)]);
+            }
+            const double m = B.mass[gb];
+            const double* I = B.inertia + 6 * gb;
+            acc[1] += 1;
+            acc[2] += 3 * m + (I[0] + I[1] + I[2]);  // genMassMat().trace()
+            acc[3] += spd * m;
+            acc[4] += m;
+        }
+        red.sum(acc);
+        n_local = (int)acc[0];
+        n_active = (int)acc[1];
+        cm = (n_active > 0) ? acc[2] / n_active / 6 : 1;  // :36
+        double csv = acc[3] / acc[4];                    // :72
+        double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+        csv = dmax(csv, gn * dt * 0.25);
+        csv = dmax(csv, 1e-4);
+        cs = csv;
+        // dense direct solve for small scenes on the direct branch (LDLT analogue)
+        dense_mode = B.dense != nullptr && n_local < C.direct_threshold && C.dense_max > 0 &&
+                     n_active <= C.dense_max && n_active > 0;
+        if (dense_mode) {
+            block_scan(0, [&](int b) { return active(b0 + b) ? 1 : 0; },
+                       [&](int b, int excl) {
+                           if (active(b0 + b)) {
+                               B.didx[b0 + b] = excl;
+                               B.dbody[b0 + excl] = b0 + b;
+                           }
+                       });
+        }
+        // velocities (non-dimensional) :203-217
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            if (!B.local[gb]) continue;
+            for (int r = 0; r < 3; ++r) {
+                double v = B.vel[3 * gb + r], w = B.ang[3 * gb + r];
+                double vo = v;
+                if (!B.is_static[gb]) vo += g[r] * dt;
+                B.u[6 * gb + r] = v / cs;
+                B.u[6 * gb + 3 + r] = w / cs;
+                B.uold[6 * gb + r] = vo / cs;
+                B.uold[6 * gb + 3 + r] = w / cs;
+                B.du[6 * gb + r] = 0;
+                B.du[6 * gb + 3 + r] = 0;
+            }
+        }
+        // preprocess (NonSmoothContactForce.cpp:8-48) + initForces (:49-52)
+        const double damp = C.spring_damp * C.spring_k;
+        const double tk = dt * C.spring_k;
+        compliance = 1. / (dt * (tk + damp));
+        reduction = tk / (tk + damp);
+        spring_term = (C.spring_based ? 1.0 : 0.0) * compliance * cm;
+        __syncthreads();
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            double k = 0;
+            if (C.spring_based) {
+                k += -reduction * B.depth[gc] / dt / cs;
+            } else {
+                d3 w = rel_vel(gc, B.u);
+                k += w.x * C.restitution;
+            }
+            B.kn[gc] = k;
+            B.f[3 * gc] = 1;
+            B.f[3 * gc + 1] = 0;
+            B.f[3 * gc + 2] = 0;
+            B.lam[2 * gc] = 1e-2;
+            B.lam[2 * gc + 1] = 1e-2;
+        }
+        __syncthreads();
+        return true;
+    }
+
+    // toLocal(vels) = -T0^T u0 - T1^T u1 = R^T[(v1 + w1 x c1) - (v0 + w0 x c0)]
+    // (ContactInfo.h:46-51); non-local/static bodies read their (fixed) u.
+    __device__ __forceinline__ d3 rel_vel(int gc, const double* uvec) const {
+        const Frame R = ld_frame(B.frame + 9 * gc);
+        const int gb0 = b0 + B.cbody[2 * gc], gb1 = b0 + B.cbody[2 * gc + 1];
+        d3 p0 = point_vel(uvec + 6 * gb0, ld3(B.arm + 6 * gc));
+        d3 p1 = point_vel(uvec + 6 * gb1, ld3(B.arm + 6 * gc + 3));
+        return to_frame(R, sub3(p1, p0));
+    }
+
+    // Tangential weight (calculateTangentialWeight, NonSmoothContactForce.cpp:74-104)
+    __device__ __forceinline__ double tangential_weight(int gc, const Frame& R, d3 w, double fn) const {
+        const double tn = sqrt(w.y * w.y + w.z * w.z);
+        double th0 = w.y, th1 = w.z;
+        if (tn > 0) { th0 = w.y / tn; th1 = w.z / tn; }
+        // world tangent direction d = R (0, th0, th1); hh_j = T_j[:,1:] th = s_j [d; c_j x d]
+        d3 d = from_frame(R, d3{0.0, th0, th1});
+        double fw = 0;
+        for (int j = 0; j < 2; ++j) {
+            const int gb = b0 + B.cbody[2 * gc + j];
+            if (B.is_static[gb]) continue;
+            d3 c = ld3(B.arm + 6 * gc + 3 * j);
+            d3 t = cross3(c, d);
+            const double im = 1.0 / B.mass[gb];
+            const double* J = B.inv_inertia + 6 * gb;
+            d3 Jt = d3{J[0] * t.x + J[3] * t.y + J[4] * t.z, J[3] * t.x + J[1] * t.y + J[5] * t.z,
+                       J[4] * t.x + J[5] * t.y + J[2] * t.z};
+            const double q = im * dot3(d, d) + dot3(t, Jt);
+            fw += q * cm;
+        }
+        const double rad = cone_radius(fn, cmu(gc));
+        return dmin(rad / (tn + 1e-8) * fw, 1.0);
+    }
+
+    // Residual terms of one contact at state (uvec, f, lam) (nonSmoothResiduals :119-172,
+    // ACVector :53-73).  Writes X = -R f for the ru gather; returns squared norms.
+    __device__ __forceinline__ void contact_residual(int gc, const double* uvec, const double* fv, const double* lv,
+                                                     bool stored, double muc, double* rf_out, double* rl_out,
+                                                     double& wrf2, double& rl2, double& ac2) const {
+        const Frame R = ld_frame(B.frame + 9 * gc);
+        const d3 w = rel_vel(gc, uvec);
+        const double fn = fv[0], f1 = fv[1], f2 = fv[2];
+        const double mu = cmu(gc);
+        double g0, g1;
+        if (stored) { g0 = B.gr[2 * gc]; g1 = B.gr[2 * gc + 1]; }
+        else cone_grad(f1, f2, g0, g1);
+        double r0 = 0 - w.x, r1 = 0 - w.y, r2 = 0 - w.z;
+        if (C.spring_based) r0 -= compliance * cm * fn;
+        r0 += lv[0];
+        r1 -= lv[1] * g0;
+        r2 -= lv[1] * g1;
+        r0 -= B.kn[gc];
+        double cn, cc;
+        if (stored) { cn = B.cv[2 * gc]; cc = B.cv[2 * gc + 1]; }
+        else { cn = -fn; cc = cone_c(fn, f1, f2, mu); }
+        const double rl0 = lv[0] * cn + muc, rl1 = lv[1] * cc + muc;
+        const double wt = tangential_weight(gc, R, w, fn);
+        const double w1 = r1 * wt, w2 = r2 * wt;
+        wrf2 += r0 * r0 + w1 * w1 + w2 * w2;
+        rl2 += rl0 * rl0 + rl1 * rl1;
+        // Alart-Curnier (:60-70)
+        const double tp = fn - (w.x + B.kn[gc] + spring_term * fn);
+        const double a0 = dmax(tp, 0.0) - fn;
+        const double rad = cone_radius(fn, mu);
+        const double td0 = f1 - w.y, td1 = f2 - w.z;
+        const double tdn = sqrt(td0 * td0 + td1 * td1);
+        double p0 = td0, p1 = td1;
+        if (!(tdn < rad)) { p0 = td0 * rad / tdn; p1 = td1 * rad / tdn; }
+        const double a1 = p0 - f1, a2 = p1 - f2;
+        ac2 += a0 * a0 + a1 * a1 + a2 * a2;
+        if (rf_out) { rf_out[0] = r0; rf_out[1] = r1; rf_out[2] = r2; }
+        if (rl_out) { rl_out[0] = rl0; rl_out[1] = rl1; }
+        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
+    }
+
+    // ru = M(u - uold) (+ gather of T_j f); static rows zero (calculateResiduals :151-163)
+    __device__ __forceinline__ void body_residual(int gb, const double* ub, double* ru_out, double& ru2) const {
+        double d[6], y[6], gth[6];
+        for (int r = 0; r < 6; ++r) d[r] = ub[r] - B.uold[6 * gb + r];
+        mass_mul(gb, d, y);
+        gather(gb, gth);
+        for (int r = 0; r < 6; ++r) {
+            const double v = y[r] + gth[r];
+            ru2 += v * v;
+            if (ru_out) ru_out[r] = v;
+        }
+    }
+
+    // ------------------------------------------------------------ Newton
+    __device__ void newton(pdc_stats& st) {
+        const int n_rigid = 6 * n_local, n_force = 3 * nc, n_cons = 2 * nc;
+        const bool direct = n_local < C.direct_threshold;
+        double Hu = 1e-4, exitErr = 0;
+        const double power = 0.66667;
+        int it = 0, pcg_total = 0, ls_total = 0, gd_total = 0;
+        bool ls_fail = false, nonfinite = false;
+        for (it = 0; it < C.max_iter; ++it) {
+            t_mark = now();
+            // calculateConstraints (:105-118) + surrogateDualGap
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int c = tid; c < nc; c += nt) {
+                const int gc = c0 + c;
+                const double fn = B.f[3 * gc], f1 = B.f[3 * gc + 1], f2 = B.f[3 * gc + 2];
+                const double cn = -fn, cc = cone_c(fn, f1, f2, cmu(gc));
+                B.cv[2 * gc] = cn;
+                B.cv[2 * gc + 1] = cc;
+                double g0, g1, h0, h1, h2;
+                cone_grad(f1, f2, g0, g1);
+                cone_hess(f1, f2, h0, h1, h2);
+                B.gr[2 * gc] = g0;
+                B.gr[2 * gc + 1] = g1;
+                B.hs[3 * gc] = h0;
+                B.hs[3 * gc + 1] = h1;
+                B.hs[3 * gc + 2] = h2;
+                acc[0] += B.lam[2 * gc] * cn + B.lam[2 * gc + 1] * cc;
+            }
+            red.sum(acc);
+            const double sDualGap = -(acc[0] / n_cons);
+            const double muc = sDualGap * 0.1;
+            // residuals at the current iterate (:292-300)
+            double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2
+            for (int c = tid; c < nc; c += nt) {
+                const int gc = c0 + c;
+                contact_residual(gc, B.u, B.f + 3 * gc, B.lam + 2 * gc, true, muc, B.rf + 3 * gc, B.rl + 2 * gc,
+                                 e[1], e[2], e[3]);
+            }
+            __syncthreads();
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!B.local[gb]) continue;
+                if (B.is_static[gb]) {
+                    for (int r = 0; r < 6; ++r) B.ru[6 * gb + r] = 0;
+                    continue;
+                }
+                body_residual(gb, B.u + 6 * gb, B.ru + 6 * gb, e[0]);
+            }
+            red.sum(e);
+            const double err = e[0] + e[1] + e[2];
+            const double sErr = err, sacErr = e[0] + e[3] + e[2];
+            const double eps = Hu * pow(err, power * 0.5);
+            const double momenErr = sqrt(e[0]) / n_rigid;
+            exitErr = dmax(momenErr, sqrt(e[1]) / n_force);
+            exitErr = dmax(exitErr, sqrt(e[2]) / n_cons);
+            exitErr = dmax(exitErr, sDualGap);
+            exitErr = dmin(exitErr, dmax(momenErr, sqrt(e[3]) / nc));
+            if (exitErr < C.tol) break;
+
+            // linsysAddition (:173-253): per-contact K, K^-1, sf, W, rhs vector
+            for (int c = tid; c < nc; c += nt) {
+                const int gc = c0 + c;
+                const double ln = B.lam[2 * gc], lt = B.lam[2 * gc + 1];
+                const double ic0 = 1. / (B.cv[2 * gc] - eps * ln);
+                const double ic1 = 1. / (B.cv[2 * gc + 1] - eps * lt);
+                B.invC[2 * gc] = ic0;
+                B.invC[2 * gc + 1] = ic1;
+                const double g0 = B.gr[2 * gc], g1 = B.gr[2 * gc + 1];
+                double lNorm = -ln * ic0;
+                if (C.spring_based) lNorm += compliance * cm;
+                const double rl0 = B.rl[2 * gc], rl1 = B.rl[2 * gc + 1];
+                const double a = -lt * ic1;
+                const double sf0 = B.rf[3 * gc] + (-rl0 * ic0);
+                const double sf1 = B.rf[3 * gc + 1] + g0 * rl1 * ic1;
+                const double sf2 = B.rf[3 * gc + 2] + g1 * rl1 * ic1;
+                B.sf[3 * gc] = sf0;
+                B.sf[3 * gc + 1] = sf1;
+                B.sf[3 * gc + 2] = sf2;
+                const double kni = 1. / (eps + lNorm);
+                B.knInv[gc] = kni;
+                const double k00 = eps + a * g0 * g0 + lt * B.hs[3 * gc];
+                const double k01 = 0 + a * g0 * g1 + lt * B.hs[3 * gc + 1];
+                const double k11 = eps + a * g1 * g1 + lt * B.hs[3 * gc + 2];
+                const double det = k00 * k11 - k01 * k01;
+                const double t00 = k11 / det, t01 = -k01 / det, t11 = k00 / det;
+                B.ktInv[3 * gc] = t00;
+                B.ktInv[3 * gc + 1] = t01;
+                B.ktInv[3 * gc + 2] = t11;
+                const Frame R = ld_frame(B.frame + 9 * gc);
+                frame_sandwich(R, kni, t00, t01, t11, B.W + 6 * gc);
+                const d3 ks = d3{sf0 * kni, t00 * sf1 + t01 * sf2, t01 * sf1 + t11 * sf2};
+                st3(B.X + 3 * gc, from_frame(R, ks));
+            }
+            __syncthreads();
+            // rhs = sum getTrans(j) K^-1 sf - ru; block-Jacobi blocks; PCG start
+            double rr[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // r.z, b.b
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                double gth[6];
+                gather(gb, gth);
+                double* rb = B.rhs + 6 * gb;
+                for (int r = 0; r < 6; ++r) rb[r] = gth[r] - B.ru[6 * gb + r];
+                // diagonal block: M/cm + eps I + sum_j T_j K^-1 T_j^T
+                double P[21];
+                for (int q = 0; q < 21; ++q) P[q] = 0;
+                {
+                    const double m = B.mass[gb] / cm;
+                    const double* I = B.inertia + 6 * gb;
+                    P[pk(0, 0)] = m + eps;
+                    P[pk(1, 1)] = m + eps;
+                    P[pk(2, 2)] = m + eps;
+                    P[pk(3, 3)] = I[0] / cm + eps;
+                    P[pk(4, 4)] = I[1] / cm + eps;
+                    P[pk(5, 5)] = I[2] / cm + eps;
+                    P[pk(4, 3)] = I[3] / cm;
+                    P[pk(5, 3)] = I[4] / cm;
+                    P[pk(5, 4)] = I[5] / cm;
+                }
+                const int st0 = B.inc_start[gb], n = B.inc_cnt[gb];
+                for (int k = 0; k < n; ++k) {
+                    const int e2 = B.inc[st0 + k];
+                    const int gc = e2 >> 1, side = e2 & 1;
+                    const double* W = B.W + 6 * gc;
+                    const d3 c = ld3(B.arm + 6 * gc + 3 * side);
+                    // Y = C W (C = [c]x): column k of Y = c x W_col_k
+                    const d3 wc0 = d3{W[0], W[3], W[4]}, wc1 = d3{W[3], W[1], W[5]}, wc2 = d3{W[4], W[5], W[2]};
+                    const d3 y0 = cross3(c, wc0), y1 = cross3(c, wc1), y2 = cross3(c, wc2);
+                    // Z = C Y^T: column k of Z = c x (row k of Y)
+                    const d3 z0 = cross3(c, d3{y0.x, y1.x, y2.x});
+                    const d3 z1 = cross3(c, d3{y0.y, y1.y, y2.y});
+                    const d3 z2 = cross3(c, d3{y0.z, y1.z, y2.z});
+                    P[pk(0, 0)] += W[0]; P[pk(1, 0)] += W[3]; P[pk(1, 1)] += W[1];
+                    P[pk(2, 0)] += W[4]; P[pk(2, 1)] += W[5]; P[pk(2, 2)] += W[2];
+                    P[pk(3, 0)] += y0.x; P[pk(3, 1)] += y1.x; P[pk(3, 2)] += y2.x;
+                    P[pk(4, 0)] += y0.y; P[pk(4, 1)] += y1.y; P[pk(4, 2)] += y2.y;
+                    P[pk(5, 0)] += y0.z; P[pk(5, 1)] += y1.z; P[pk(5, 2)] += y2.z;
+                    P[pk(3, 3)] += z0.x; P[pk(4, 3)] += z0.y; P[pk(4, 4)] += z1.y;
+                    P[pk(5, 3)] += z0.z; P[pk(5, 4)] += z1.z; P[pk(5, 5)] += z2.z;
+                }
+                if (dense_mode) {
+                    assemble_dense_rows(gb, P);
+                } else {
+                    double* Pi = B.pinv + 21 * gb;
+                    if (!spd6_inverse(P, Pi)) {
+                        for (int q = 0; q < 21; ++q) Pi[q] = 0;
+                        for (int r = 0; r < 6; ++r) Pi[pk(r, r)] = 1.0 / P[pk(r, r)];
+                    }
+                }
+                for (int r = 0; r < 6; ++r) rr[1] += rb[r] * rb[r];
+            }
+            red.sum(rr);  // sync: rhs, pinv complete
+            const double bnorm = sqrt(rr[1]);
+            unsigned long long t1 = now();
+            t_build += t1 - t_mark;
+            t_mark = t1;
+
+            // ---- linear solve: block-Jacobi PCG (replaces LDLT / AMGCL, :385-427)
+            const double rtol = direct ? C.rtol_direct : C.rtol_iter;
+            const int maxit = direct ? C.max_direct : C.max_cg;
+            int iters = 0;
+            bool lin_bad = false;
+            if (dense_mode) {
+                lin_bad = !dense_solve();
+            } else {
+            if (!direct) {  // AMGCL starts from the previous du (:406-415)
+                spmv_to_X(B.du, nullptr, 0.0);
+                __syncthreads();
+            }
+            double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                double r6[6];
+                if (direct) {
+                    for (int r = 0; r < 6; ++r) { r6[r] = B.rhs[6 * gb + r]; B.du[6 * gb + r] = 0; }
+                } else {
+                    double q6[6];
+                    spmv_body(gb, B.du + 6 * gb, eps, q6);
+                    for (int r = 0; r < 6; ++r) r6[r] = B.rhs[6 * gb + r] - q6[r];
+                }
+                double z6[6];
+                prec(gb, r6, z6);
+                for (int r = 0; r < 6; ++r) {
+                    B.r[6 * gb + r] = r6[r];
+                    B.z[6 * gb + r] = z6[r];
+                    B.p[6 * gb + r] = 0;
+                    s2[0] += r6[r] * z6[r];
+                    s2[1] += r6[r] * r6[r];
+                }
+            }
+            red.sum(s2);
+            double rz = s2[0];
+            double res = (bnorm > 0) ? sqrt(s2[1]) / bnorm : 0.0;
+            double beta = 0;
+            if (bnorm == 0) {
+                // zero right-hand side: du = x0 (zero on the direct branch)
+            } else if (!(res < rtol)) {
+                for (iters = 0; iters < maxit;) {
+                    // contact phase: p_new = z + beta p for both bodies; X = W dv(p_new)
+                    spmv_to_X(B.p, B.z, beta);
+                    __syncthreads();
+                    double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    for (int b = tid; b < nb; b += nt) {
+                        const int gb = b0 + b;
+                        if (!active(gb)) continue;
+                        double pn[6], q6[6];
+                        for (int r = 0; r < 6; ++r) {
+                            pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, B.p[6 * gb + r]));
+                            B.p[6 * gb + r] = pn[r];
+                        }
+                        spmv_body(gb, pn, eps, q6);
+                        for (int r = 0; r < 6; ++r) {
+                            s3[0] += pn[r] * q6[r];
+                            B.z[6 * gb + r] = q6[r];  // z holds q until the update below
+                        }
+                    }
+                    red.sum(s3);
+                    const double alpha = rz / s3[0];
+                    double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    for (int b = tid; b < nb; b += nt) {
+                        const int gb = b0 + b;
+                        if (!active(gb)) continue;
+                        double r6[6], z6[6];
+                        for (int r = 0; r < 6; ++r) {
+                            B.du[6 * gb + r] += alpha * B.p[6 * gb + r];
+                            r6[r] = B.r[6 * gb + r] - alpha * B.z[6 * gb + r];
+                            B.r[6 * gb + r] = r6[r];
+                        }
+                        prec(gb, r6, z6);
+                        for (int r = 0; r < 6; ++r) {
+                            B.z[6 * gb + r] = z6[r];
+                            s4[0] += r6[r] * r6[r];
+                            s4[1] += r6[r] * z6[r];
+                        }
+                    }
+                    red.sum(s4);
+                    ++iters;
+                    res = sqrt(s4[0]) / bnorm;
+                    if (!(res >= rtol)) break;  // converged or non-finite
+                    beta = s4[1] / rz;
+                    rz = s4[1];
+                }
+            }
+            pcg_total += iters;
+            if (!isfinite(res)) lin_bad = true;
+            }  // PCG branch
+            if (lin_bad) {  // LDLT failure analogue (:390-394): du = 0
+                nonfinite = true;
+                for (int b = tid; b < nb; b += nt) {
+                    const int gb = b0 + b;
+                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = 0;
+                }
+            }
+            __syncthreads();
+            // retrieveNonSmoothForceInc (:254-280)
+            for (int c = tid; c < nc; c += nt) {
+                const int gc = c0 + c;
+                const d3 w = rel_vel(gc, B.du);
+                double d0 = B.sf[3 * gc] - w.x, d1 = B.sf[3 * gc + 1] - w.y, d2 = B.sf[3 * gc + 2] - w.z;
+                d0 = B.knInv[gc] * d0;
+                const double t00 = B.ktInv[3 * gc], t01 = B.ktInv[3 * gc + 1], t11 = B.ktInv[3 * gc + 2];
+                const double e1 = t00 * d1 + t01 * d2, e2 = t01 * d1 + t11 * d2;
+                B.df[3 * gc] = d0;
+                B.df[3 * gc + 1] = e1;
+                B.df[3 * gc + 2] = e2;
+                B.dl[2 * gc] = -B.invC[2 * gc] * (-B.lam[2 * gc] * d0 + B.rl[2 * gc]);
+                B.dl[2 * gc + 1] = -B.invC[2 * gc + 1] *
+                                   (B.lam[2 * gc + 1] * (B.gr[2 * gc] * e1 + B.gr[2 * gc + 1] * e2) + B.rl[2 * gc + 1]);
+            }
+            __syncthreads();
+            t1 = now();
+            t_solve += t1 - t_mark;
+            t_mark = t1;
+
+            // line search (:437-440), gradient-descent fallback (:444-467)
+            int trials = 0;
+            double step = line_search(sErr, sacErr, muc, 10, trials);
+            ls_total += trials;
+            bool useGD = false;
+            if (step == 0) {
+                useGD = true;
+                gd_total++;
+                for (int b = tid; b < nb; b += nt) {
+                    const int gb = b0 + b;
+                    if (!B.local[gb]) continue;
+                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = -B.ru[6 * gb + r];
+                }
+                for (int c = tid; c < nc; c += nt) {
+                    const int gc = c0 + c;
+                    for (int r = 0; r < 3; ++r) B.df[3 * gc + r] = B.rf[3 * gc + r];
+                    B.dl[2 * gc] = B.rl[2 * gc];
+                    B.dl[2 * gc + 1] = B.rl[2 * gc + 1];
+                }
+                __syncthreads();
+                step = line_search(sErr, sacErr, muc, 20, trials);
+                ls_total += trials;
+                if (step == 0) ls_fail = true;
+            }
+            // Hu update (:474-483)
+            if (!useGD && step == 1) {
+                if (!direct && iters == maxit) Hu *= 1.3;
+                else Hu /= 4;
+            } else {
+                Hu *= 4;
+            }
+            Hu = dmax(Hu, 1e-6);
+            t1 = now();
+            t_ls += t1 - t_mark;
+        }
+        st.newton_iters = it;
+        st.exit_err = exitErr;
+        st.pcg_iters = pcg_total;
+        st.ls_trials = ls_total;
+        st.gd_fallbacks = gd_total;
+        int stt = status;
+        if (it >= C.max_iter) stt |= PDC_SCENE_MAX_ITER;
+        if (ls_fail) stt |= PDC_SCENE_LS_FAIL;
+        if (nonfinite || !isfinite(exitErr)) stt |= PDC_SCENE_NONFINITE;
+        status = stt;
+    }
+
+    // ---------------------------------------------- dense direct solve (small scenes)
+    __device__ __forceinline__ double* dense_A() const { return B.dense + (long long)blockIdx.x * B.dense_stride; }
+
+    // Row-block of active body gb in the dense Newton matrix: the diagonal block P
+    // and, per incidence, the off-diagonal block T_b K^-1 T_o^T =
+    // -[[W, W C_o^T], [C_b W, C_b W C_o^T]] (the 4 blocks of linsysAddition, :232-247).
+    __device__ void assemble_dense_rows(int gb, const double* P) const {
+        const int n6 = 6 * n_active;
+        const int ib = B.didx[gb];
+        double* rows = dense_A() + (long long)(6 * ib) * n6;
+        for (int r = 0; r < 6; ++r)
+            for (int j = 0; j < n6; ++j) rows[r * n6 + j] = 0.0;
+        for (int r = 0; r < 6; ++r)
+            for (int c = 0; c < 6; ++c) rows[r * n6 + 6 * ib + c] = P[pk(r, c)];
+        const int st0 = B.inc_start[gb], n = B.inc_cnt[gb];
+        for (int k = 0; k < n; ++k) {
+            const int e2 = B.inc[st0 + k];
+            const int gc = e2 >> 1, side = e2 & 1;
+            const int go = b0 + B.cbody[2 * gc + (1 - side)];
+            if (!active(go) || go == gb) continue;
+            const int io = B.didx[go];
+            const double* W = B.W + 6 * gc;
+            const d3 cb = ld3(B.arm + 6 * gc + 3 * side);
+            const d3 co = ld3(B.arm + 6 * gc + 3 * (1 - side));
+            const d3 wr[3] = {d3{W[0], W[3], W[4]}, d3{W[3], W[1], W[5]}, d3{W[4], W[5], W[2]}};
+            const d3 y0 = cross3(cb, wr[0]), y1 = cross3(cb, wr[1]), y2 = cross3(cb, wr[2]);
+            const d3 yr[3] = {d3{y0.x, y1.x, y2.x}, d3{y0.y, y1.y, y2.y}, d3{y0.z, y1.z, y2.z}};
+            for (int i = 0; i < 3; ++i) {
+                const d3 tr = cross3(co, wr[i]);
+                double* row = rows + (long long)i * n6 + 6 * io;
+                row[0] -= wr[i].x; row[1] -= wr[i].y; row[2] -= wr[i].z;
+                row[3] -= tr.x; row[4] -= tr.y; row[5] -= tr.z;
+                const d3 br = cross3(co, yr[i]);
+                row = rows + (long long)(3 + i) * n6 + 6 * io;
+                row[0] -= yr[i].x; row[1] -= yr[i].y; row[2] -= yr[i].z;
+                row[3] -= br.x; row[4] -= br.y; row[5] -= br.z;
+            }
+        }
+    }
+
+    // Jacobi-scaled dense Cholesky solve of the Newton system (stands in for the
+    // SimplicialLDLT of the direct branch, :359-394).  Writes du; returns false on
+    // a non-positive pivot (the caller then sets du = 0, as :390-394).
+    __device__ bool dense_solve() {
+        const int n = 6 * n_active;
+        const int NM = 6 * C.dense_max;
+        double* A = dense_A();
+        double* x = A + (long long)NM * NM;
+        double* y = x + NM;
+        double* D = y + NM;
+        for (int i = tid; i < n; i += nt) {
+            const int gb = B.dbody[b0 + i / 6];
+            const double d = 1 / sqrt(A[(long long)i * n + i]);
+            D[i] = d;
+            x[i] = B.rhs[6 * gb + i % 6] * d;
+        }
+        __syncthreads();
+        for (long long idx = tid; idx < (long long)n * n; idx += nt) {
+            const int i = (int)(idx / n), j = (int)(idx % n);
+            A[idx] *= D[i] * D[j];
+        }
+        __syncthreads();
+        bool ok = true;
+        for (int k = 0; k < n; ++k) {
+            const double akk = A[(long long)k * n + k];
+            if (!(akk > 0)) { ok = false; break; }
+            const double inv = 1.0 / akk;
+            for (int i = k + 1 + tid; i < n; i += nt) {
+                double* Ai = A + (long long)i * n;
+                const double aik = Ai[k] * inv;
+                for (int j = k + 1; j <= i; ++j) Ai[j] -= aik * A[(long long)j * n + k];
+            }
+            __syncthreads();
+        }
+        if (ok) {
+            for (int k = tid; k < n; k += nt) y[k] = sqrt(A[(long long)k * n + k]);
+            __syncthreads();
+            for (int i = tid; i < n; i += nt)
+                for (int k = 0; k <= i; ++k) {
+                    double& a = A[(long long)i * n + k];
+                    a = (i == k) ? y[k] : a / y[k];
+                }
+            __syncthreads();
+            for (int k = 0; k < n; ++k) {  // L y = x
+                const double yk = x[k] / A[(long long)k * n + k];
+                if (tid == 0) y[k] = yk;
+                for (int i = k + 1 + tid; i < n; i += nt) x[i] -= A[(long long)i * n + k] * yk;
+                __syncthreads();
+            }
+            for (int k = n - 1; k >= 0; --k) {  // L^T z = y
+                const double* Ak = A + (long long)k * n;
+                const double zk = y[k] / Ak[k];
+                if (tid == 0) x[k] = zk;
+                for (int i = tid; i < k; i += nt) y[i] -= Ak[i] * zk;
+                __syncthreads();
+            }
+            for (int i = tid; i < n; i += nt) {
+                const int gb = B.dbody[b0 + i / 6];
+                B.du[6 * gb + i % 6] = x[i] * D[i];
+            }
+        }
+        __syncthreads();
+        return ok;
+    }
+
+    // X = W (v1p - v0p) of direction vec (or of z + beta*vec when zvec != null),
+    // with the direction of static / non-active bodies taken as zero.
+    __device__ __forceinline__ void spmv_to_X(const double* vec, const double* zvec, double beta) const {
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            d3 pv[2];
+            for (int j = 0; j < 2; ++j) {
+                const int gb = b0 + B.cbody[2 * gc + j];
+                if (B.is_static[gb]) { pv[j] = d3{0, 0, 0}; continue; }
+                double pn[6];
+                if (zvec) {
+                    for (int r = 0; r < 6; ++r) pn[r] = __dadd_rn(zvec[6 * gb + r], __dmul_rn(beta, vec[6 * gb + r]));
+                } else {
+                    for (int r = 0; r < 6; ++r) pn[r] = vec[6 * gb + r];
+                }
+                pv[j] = point_vel(pn, ld3(B.arm + 6 * gc + 3 * j));
+            }
+            st3(B.X + 3 * gc, sym_mul(B.W + 6 * gc, sub3(pv[1], pv[0])));
+        }
+    }
+    // (M/cm + eps I) x + gather(X)  for one active body
+    __device__ __forceinline__ void spmv_body(int gb, const double* x6, double eps, double* q6) const {
+        double y[6], gth[6];
+        mass_mul(gb, x6, y);
+        gather(gb, gth);
+        for (int r = 0; r < 6; ++r) q6[r] = y[r] + eps * x6[r] + gth[r];
+    }
+    __device__ __forceinline__ void prec(int gb, const double* r6, double* z6) const {
+        const double* Pi = B.pinv + 21 * gb;
+        for (int a = 0; a < 6; ++a) {
+            double s = 0;
+            for (int c = 0; c < 6; ++c) s += Pi[pk(a, c)] * r6[c];
+            z6[a] = s;
+        }
+    }
+
+    // filterLineSearch (NonSmoothContactForce.cpp:281-319) applied to step*d
+    __device__ __forceinline__ void filter(int gc, double step, double* dfin, double* dlin) const {
+        const double mu = cmu(gc);
+        const double cf0 = B.f[3 * gc], cf1 = B.f[3 * gc + 1], cf2 = B.f[3 * gc + 2];
+        dfin[0] = step * B.df[3 * gc];
+        dfin[1] = step * B.df[3 * gc + 1];
+        dfin[2] = step * B.df[3 * gc + 2];
+        double t0 = cf0 + dfin[0], t1 = cf1 + dfin[1], t2 = cf2 + dfin[2];
+        if (t0 < 0) {
+            t0 = 0;
+            dfin[0] = t0 - cf0;
+            dfin[1] = t1 - cf1;
+            dfin[2] = t2 - cf2;
+        }
+        if (cone_c(t0, t1, t2, mu) > 0) {
+            // project(tf, tf) (LorentzCircleConstraint.cpp:36-49)
+            double o0 = t0, o1 = t1, o2 = t2;
+            if (t0 < 0) o0 = 0;
+            if (cone_c(o0, o1, o2, mu) > 0) {
+                const double rad = dmax(cone_radius(t0, mu) + 0, 0.0);
+                const double s = rad / sqrt(o1 * o1 + o2 * o2);
+                o1 *= s;
+                o2 *= s;
+            }
+            dfin[0] = o0 - cf0;
+            dfin[1] = o1 - cf1;
+            dfin[2] = o2 - cf2;
+        }
+        for (int k = 0; k < 2; ++k) {
+            double d = step * B.dl[2 * gc + k];
+            const double l = B.lam[2 * gc + k];
+            if (d < 0 && l + d < 0) d = -l;
+            dlin[k] = d;
+        }
+    }
+
+    // lineSearch (PrimalDualForceSolver.cpp:562-635).  Commits the accepted
+    // trial into (u, f, lam) and returns the step (0 = nothing accepted).
+    __device__ double line_search(double sErr, double sacErr, double muc, int maxLS, int& trials) {
+        double step = 1.0;
+        trials = 0;
+        for (int t = 0; t < maxLS; ++t) {
+            ++trials;
+            double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2, du.ru, df.rf, (dl/l).rl
+            for (int c = tid; c < nc; c += nt) {
+                const int gc = c0 + c;
+                double dfin[3], dlin[2], fI[3], lI[2];
+                filter(gc, step, dfin, dlin);
+                for (int k = 0; k < 2; ++k) lI[k] = __dadd_rn(B.lam[2 * gc + k], __dmul_rn(0.99, dlin[k]));
+                for (int k = 0; k < 3; ++k) fI[k] = __dadd_rn(B.f[3 * gc + k], __dmul_rn(0.99, dfin[k]));
+                for (int k = 0; k < 3; ++k) B.fT[3 * gc + k] = fI[k];
+                for (int k = 0; k < 2; ++k) B.lT[2 * gc + k] = lI[k];
+                // residual at the trial point with velocities u + 0.99 step du (both bodies)
+                const Frame R = ld_frame(B.frame + 9 * gc);
+                d3 pv[2];
+                for (int j = 0; j < 2; ++j) {
+                    const int gb = b0 + B.cbody[2 * gc + j];
+                    double ui[6];
+                    trial_u(gb, step, ui);
+                    pv[j] = point_vel(ui, ld3(B.arm + 6 * gc + 3 * j));
+                }
+                const d3 w = to_frame(R, sub3(pv[1], pv[0]));
+                double rfv[3], rlv[2];
+                contact_residual_w(gc, R, w, fI, lI, muc, rfv, rlv, e[1], e[2], e[3]);
+                e[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
+                e[6] += (dlin[0] / lI[0]) * rlv[0] + (dlin[1] / lI[1]) * rlv[1];
+            }
+            __syncthreads();
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                double ui[6], ruv[6];
+                trial_u(gb, step, ui);
+                double r2 = 0;
+                body_residual(gb, ui, ruv, r2);
+                e[0] += r2;
+                for (int r = 0; r < 6; ++r) e[4] += (step * B.du[6 * gb + r]) * ruv[r];
+            }
+            red.sum(e);
+            const double inErr = e[0] + e[1] + e[2];
+            const double sacIn = e[0] + e[3] + e[2];
+            const double gErr = -e[4] + e[5] + e[6];
+            const bool acpt = (inErr < sErr) | (sacIn < sacErr);
+            if ((acpt && gErr > 0) || (t == maxLS - 1)) {
+                if (acpt) {
+                    for (int b = tid; b < nb; b += nt) {
+                        const int gb = b0 + b;
+                        if (!B.local[gb]) continue;
+                        double ui[6];
+                        trial_u(gb, step, ui);
+                        for (int r = 0; r < 6; ++r) B.u[6 * gb + r] = ui[r];
+                    }
+                    for (int c = tid; c < nc; c += nt) {
+                        const int gc = c0 + c;
+                        for (int k = 0; k < 3; ++k) B.f[3 * gc + k] = B.fT[3 * gc + k];
+                        for (int k = 0; k < 2; ++k) B.lam[2 * gc + k] = B.lT[2 * gc + k];
+                    }
+                    __syncthreads();
+                    return step;
+                }
+                break;
+            }
+            step *= 0.5;
+        }
+        return 0.0;
+    }
+    __device__ __forceinline__ void trial_u(int gb, double step, double* ui) const {
+        for (int r = 0; r < 6; ++r)
+            ui[r] = __dadd_rn(B.u[6 * gb + r], __dmul_rn(0.99, __dmul_rn(step, B.du[6 * gb + r])));
+    }
+    // contact residual with fresh constraints, given the relative velocity w
+    __device__ __forceinline__ void contact_residual_w(int gc, const Frame& R, d3 w, const double* fv,
+                                                       const double* lv, double muc, double* rfo, double* rlo,
+                                                       double& wrf2, double& rl2, double& ac2) const {
+        const double fn = fv[0], f1 = fv[1], f2 = fv[2];
+        const double mu = cmu(gc);
+        double g0, g1;
+        cone_grad(f1, f2, g0, g1);
+        double r0 = 0 - w.x, r1 = 0 - w.y, r2 = 0 - w.z;
+        if (C.spring_based) r0 -= compliance * cm * fn;
+        r0 += lv[0];
+        r1 -= lv[1] * g0;
+        r2 -= lv[1] * g1;
+        r0 -= B.kn[gc];
+        const double rl0 = lv[0] * (-fn) + muc, rl1 = lv[1] * cone_c(fn, f1, f2, mu) + muc;
+        const double wt = tangential_weight(gc, R, w, fn);
+        const double w1 = r1 * wt, w2 = r2 * wt;
+        wrf2 += r0 * r0 + w1 * w1 + w2 * w2;
+        rl2 += rl0 * rl0 + rl1 * rl1;
+        const double tp = fn - (w.x + B.kn[gc] + spring_term * fn);
+        const double a0 = dmax(tp, 0.0) - fn;
+        const double rad = cone_radius(fn, mu);
+        const double td0 = f1 - w.y, td1 = f2 - w.z;
+        const double tdn = sqrt(td0 * td0 + td1 * td1);
+        double p0 = td0, p1 = td1;
+        if (!(tdn < rad)) { p0 = td0 * rad / tdn; p1 = td1 * rad / tdn; }
+        const double a1 = p0 - f1, a2 = p1 - f2;
+        ac2 += a0 * a0 + a1 * a1 + a2 * a2;
+        rfo[0] = r0; rfo[1] = r1; rfo[2] = r2;
+        rlo[0] = rl0; rlo[1] = rl1;
+        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
+    }
+
+    // KKT report at the final iterate (mu_c = 0) and write-back (:491-510).
+    __device__ void finish(pdc_stats& st) {
+        double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double mx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            const Frame R = ld_frame(B.frame + 9 * gc);
+            const d3 w = rel_vel(gc, B.u);
+            double rfv[3], rlv[2], d1 = 0, d2 = 0, d3v = 0;
+            contact_residual_w(gc, R, w, B.f + 3 * gc, B.lam + 2 * gc, 0.0, rfv, rlv, d1, d2, d3v);
+            e[1] += rfv[0] * rfv[0] + rfv[1] * rfv[1] + rfv[2] * rfv[2];
+            mx[0] = dmax(mx[0], dmax(fabs(rlv[0]), fabs(rlv[1])));
+            const double fn = B.f[3 * gc];
+            mx[1] = dmax(mx[1], dmax(-fn, cone_c(fn, B.f[3 * gc + 1], B.f[3 * gc + 2], cmu(gc))));
+            for (int k = 0; k < 3; ++k) B.lforce[3 * gc + k] = B.f[3 * gc + k] * cs * cm;
+        }
+        __syncthreads();
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            if (!B.local[gb]) continue;
+            if (!B.is_static[gb]) body_residual(gb, B.u + 6 * gb, nullptr, e[0]);
+            for (int r = 0; r < 3; ++r) {
+                B.dvel[3 * gb + r] = B.u[6 * gb + r] * cs - B.vel[3 * gb + r];
+                B.dang[3 * gb + r] = B.u[6 * gb + 3 + r] * cs - B.ang[3 * gb + r];
+            }
+        }
+        red.sum(e);
+        red.max(mx);
+        st.kkt_stationarity = dmax(sqrt(e[0]) / (6.0 * n_local), sqrt(e[1]) / (3.0 * nc));
+        st.kkt_complementarity = mx[0];
+        st.kkt_cone = mx[1];
+        st.char_mass = cm;
+        st.char_speed = cs;
+        st.n_local_bodies = n_local;
+        st.status = status;
+    }
+};
+
+__global__ void __launch_bounds__(256) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
+                                                           const __grid_constant__ EngineCfg C) {
+    __shared__ double s_red[2 * 8 * 32];
+    __shared__ int s_scene;
+    BlockReducer<8> red;
+    red.init(s_red);
+    for (;;) {
+        if (threadIdx.x == 0) s_scene = atomicAdd(B.work_counter, 1);
+        __syncthreads();
+        const int q = s_scene;
+        __syncthreads();
+        if (q >= B.n_scenes) break;
+        const int s = B.order ? B.order[q] : q;
+        SceneSolver S(B, C, red, s);
+        pdc_stats st;
+        st.status = 0;
+        st.newton_iters = 0;
+        st.pcg_iters = 0;
+        st.ls_trials = 0;
+        st.gd_fallbacks = 0;
+        st.n_local_bodies = 0;
+        st.exit_err = 0;
+        st.kkt_stationarity = 0;
+        st.kkt_complementarity = 0;
+        st.kkt_cone = 0;
+        st.char_mass = 0;
+        st.char_speed = 0;
+        const unsigned long long t0 = S.now();
+        if (S.setup()) {
+            S.newton(st);
+            S.finish(st);
+        } else {
+            st.status = S.status;
+        }
+        if (threadIdx.x == 0) {
+            if (B.stats) B.stats[s] = st;
+            if (B.timers) {
+                atomicAdd(&B.timers[0], S.now() - t0);
+                atomicAdd(&B.timers[1], S.t_build);
+                atomicAdd(&B.timers[2], S.t_solve);
+                atomicAdd(&B.timers[3], S.t_ls);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace pdc

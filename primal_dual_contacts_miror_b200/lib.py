@@ -1,0 +1,181 @@
+"""ctypes binding of libpdc.so (the sm_100a CUDA solver behind include/pdc.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, every entry point raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .build import LIB
+
+_lib = None
+
+
+class PdcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load libpdc.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise PdcError(abi.PDC_ENODEV, f"{LIB} not built; run primal_dual_contacts_miror_b200.build.build()")
+    lib = C.CDLL(LIB)
+    vp = C.c_void_p
+    lib.pdc_config_default.argtypes = [C.POINTER(abi.Config)]
+    lib.pdc_config_default.restype = None
+    lib.pdc_create.argtypes = [C.POINTER(abi.Config), C.POINTER(vp)]
+    lib.pdc_create.restype = C.c_int
+    lib.pdc_destroy.argtypes = [vp]
+    lib.pdc_destroy.restype = None
+    lib.pdc_reset.argtypes = [vp]
+    lib.pdc_reset.restype = C.c_int
+    lib.pdc_solve.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(abi.Bodies),
+                              C.POINTER(abi.Contacts), C.POINTER(abi.Result)]
+    lib.pdc_solve.restype = C.c_int
+    lib.pdc_solve_async.argtypes = [vp, C.c_double, C.POINTER(C.c_double), C.POINTER(abi.Bodies),
+                                    C.POINTER(abi.Contacts), C.POINTER(abi.Result), vp]
+    lib.pdc_solve_async.restype = C.c_int
+    dp = C.POINTER(C.c_double)
+    lib.pdc_batch_solve.argtypes = [vp, C.POINTER(abi.Batch), C.POINTER(abi.Bodies), C.POINTER(abi.Contacts),
+                                    dp, dp, dp, C.POINTER(abi.Stats)]
+    lib.pdc_batch_solve.restype = C.c_int
+    lib.pdc_batch_solve_async.argtypes = [vp, C.POINTER(abi.Batch), C.POINTER(abi.Bodies),
+                                          C.POINTER(abi.Contacts), dp, dp, dp, C.POINTER(abi.Stats), vp]
+    lib.pdc_batch_solve_async.restype = C.c_int
+    lib.pdc_sync.argtypes = [vp, C.c_int32]
+    lib.pdc_sync.restype = C.c_int
+    lib.pdc_timings.argtypes = [vp, dp]
+    lib.pdc_timings.restype = C.c_int
+    lib.pdc_last_error.argtypes = [vp]
+    lib.pdc_last_error.restype = C.c_char_p
+    lib.pdc_version.argtypes = []
+    lib.pdc_version.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+EXPORTED_SYMBOLS = [
+    "pdc_config_default", "pdc_create", "pdc_destroy", "pdc_reset", "pdc_solve", "pdc_solve_async",
+    "pdc_batch_solve", "pdc_batch_solve_async", "pdc_sync", "pdc_timings", "pdc_last_error", "pdc_version",
+]
+
+
+class Solver:
+    """Owner of one pdc_solver handle."""
+
+    def __init__(self, cfg=None, **overrides):
+        self.lib = load()
+        self.cfg = cfg if cfg is not None else abi.default_config(**overrides)
+        h = C.c_void_p()
+        rc = self.lib.pdc_create(C.byref(self.cfg), C.byref(h))
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pdc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(self.h).decode())
+
+    def solve(self, scene, dt=0.01, gravity=(0.0, 0.0, -9.81)):
+        """One step on one HostScene -> (dvel, dang_vel, local_force, stats)."""
+        dvel, dang, lf = abi.result_arrays(scene.n_bodies, scene.n_contacts)
+        res = abi.result_struct(dvel, dang, lf)
+        g = (C.c_double * 3)(*gravity)
+        b = scene.bodies_struct()
+        c = scene.contacts_struct()
+        self._check(self.lib.pdc_solve(self.h, dt, g, C.byref(b), C.byref(c), C.byref(res)))
+        return dvel, dang, lf, res.stats.as_dict()
+
+    def batch_solve(self, batch):
+        """All scenes of a HostBatch -> (dvel, dang_vel, local_force, [stats])."""
+        nb, nc = batch.all.n_bodies, batch.all.n_contacts
+        dvel, dang, lf = abi.result_arrays(nb, nc)
+        stats = (abi.Stats * max(batch.n_scenes, 1))()
+        b = batch.all.bodies_struct()
+        c = batch.all.contacts_struct()
+        bs = batch.batch_struct()
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.pdc_batch_solve(self.h, C.byref(bs), C.byref(b), C.byref(c), dp(dvel), dp(dang),
+                                             dp(lf), stats))
+        return dvel, dang, lf, [stats[k].as_dict() for k in range(batch.n_scenes)]
+
+    def batch_solve_device(self, dev, stream=None):
+        """Enqueue a batched solve on device arrays.  `dev` is a DeviceBatch
+        (pointers into device memory); returns immediately."""
+        self._check(self.lib.pdc_batch_solve_async(self.h, C.byref(dev.batch), C.byref(dev.bodies),
+                                                   C.byref(dev.contacts), dev.dvel, dev.dang, dev.lforce,
+                                                   dev.stats, C.c_void_p(stream or 0)))
+
+    def sync(self, timeout_ms=60000):
+        self._check(self.lib.pdc_sync(self.h, timeout_ms))
+
+    def timings(self):
+        out = (C.c_double * 6)()
+        self._check(self.lib.pdc_timings(self.h, out))
+        return {"force": out[0], "build": out[1], "solve": out[2], "line_search": out[3],
+                "newton_iters": out[4], "solves": out[5]}
+
+    def reset(self):
+        self._check(self.lib.pdc_reset(self.h))
+
+
+class DeviceBatch:
+    """A HostBatch copied to device memory (torch tensors keep the storage),
+    with the ABI structs pointing at it.  Used by pdc_batch_solve_async."""
+
+    def __init__(self, batch, device="cuda"):
+        import torch
+
+        t = lambda a, dt=None: torch.as_tensor(np.ascontiguousarray(a), device=device)
+        a = batch.all
+        self.keep = {
+            "body_off": t(batch.body_offsets), "contact_off": t(batch.contact_offsets), "dt": t(batch.dt),
+            "grav": t(batch.gravity), "vel": t(a.vel), "ang": t(a.ang_vel), "mass": t(a.mass),
+            "inertia": t(a.inertia), "inv_inertia": t(a.inv_inertia), "is_static": t(a.is_static),
+            "body": t(a.body), "frame": t(a.frame), "arm": t(a.arm), "depth": t(a.depth),
+        }
+        if a.mu is not None:
+            self.keep["mu"] = t(a.mu)
+        nb, nc = a.n_bodies, a.n_contacts
+        self.out_dvel = torch.zeros((nb, 3), dtype=torch.float64, device=device)
+        self.out_dang = torch.zeros((nb, 3), dtype=torch.float64, device=device)
+        self.out_lf = torch.zeros((nc, 3), dtype=torch.float64, device=device)
+        self.out_stats = torch.zeros((max(batch.n_scenes, 1) * C.sizeof(abi.Stats),), dtype=torch.uint8,
+                                     device=device)
+        k = self.keep
+        p = lambda x, ct=C.c_double: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(ct))
+        self.batch = abi.Batch(batch.n_scenes, p(k["body_off"], C.c_int32), p(k["contact_off"], C.c_int32),
+                               p(k["dt"]), p(k["grav"]))
+        self.bodies = abi.Bodies(nb, p(k["vel"]), p(k["ang"]), p(k["mass"]), p(k["inertia"]), p(k["inv_inertia"]),
+                                 p(k["is_static"], C.c_uint8))
+        mu = p(k["mu"]) if "mu" in k else C.cast(None, C.POINTER(C.c_double))
+        self.contacts = abi.Contacts(nc, p(k["body"], C.c_int32), p(k["frame"]), p(k["arm"]), p(k["depth"]), mu)
+        self.dvel = p(self.out_dvel)
+        self.dang = p(self.out_dang)
+        self.lforce = p(self.out_lf)
+        self.stats = C.cast(C.c_void_p(self.out_stats.data_ptr()), C.POINTER(abi.Stats))
+        self.n_scenes = batch.n_scenes
+
+    def stats_list(self):
+        raw = self.out_stats.cpu().numpy().tobytes()
+        arr = (abi.Stats * self.n_scenes).from_buffer_copy(raw[: self.n_scenes * C.sizeof(abi.Stats)])
+        return [s.as_dict() for s in arr]

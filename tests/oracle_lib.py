@@ -20,8 +20,8 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(ORACLE_SO):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True)
+    # always run make: a no-op when current, a rebuild when pdc.h changed
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
     lib = C.CDLL(ORACLE_SO)
     lib.pdc_oracle_solve.argtypes = [C.POINTER(abi.Config), C.c_double, C.POINTER(C.c_double),
                                      C.POINTER(abi.Bodies), C.POINTER(abi.Contacts),

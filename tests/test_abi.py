@@ -1,0 +1,61 @@
+"""CPU checks of the C-ABI boundary: the library builds, loads, exports every
+symbol include/pdc.h declares, and fails loudly (no CPU fallback) without a GPU."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from primal_dual_contacts_miror_b200 import abi, build, lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    out = set()
+    for name in os.listdir(os.path.join(ROOT, "include")):
+        if not name.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", name)).read()
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(pdc_\w+)\s*\(", text, re.M):
+            out.add(m.group(1))
+    return out
+
+
+def test_library_exports_every_declared_symbol():
+    build.build()
+    L = lib.load()
+    decl = declared_symbols()
+    assert "pdc_solve" in decl and "pdc_create" in decl
+    for sym in decl:
+        assert hasattr(L, sym), sym
+
+
+def test_struct_sizes_match_header_layout():
+    # the C structs are plain data; sizes pin the ctypes mirror to the header
+    assert C.sizeof(abi.Stats) == 6 * 4 + 6 * 8
+    assert C.sizeof(abi.Bodies) == 8 + 6 * 8
+    assert C.sizeof(abi.Contacts) == 8 + 5 * 8
+
+
+def test_no_device_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(lib.PdcError) as e:
+        lib.Solver()
+    assert e.value.code == abi.PDC_ENODEV
+
+
+def test_config_defaults_match_reference_yaml_defaults():
+    L = lib.load()
+    c = abi.Config()
+    L.pdc_config_default(C.byref(c))
+    assert c.max_iter == 100 and c.tol == 1e-6  # PrimalDualForceSolver.cpp:651-652
+    assert c.mu == 0.5 and c.restitution == 0.0  # NonSmoothContactForce.cpp:329-333
+    assert c.spring_k == 1e6 and c.spring_damp == 0.01
+    assert c.direct_threshold == 2000 and c.pcg_max_iter == 1000
+    py = abi.default_config()
+    for name, _ in abi.Config._fields_:
+        assert getattr(py, name) == getattr(c, name), name

@@ -1,0 +1,158 @@
+"""GPU parity of the plain FP64 path against the CPU oracle, through the C ABI.
+
+Bar: per-step body velocity increments and contact impulses within 1e-9
+(normwise relative) of the oracle and Newton iteration counts within +-1, on
+scenes where the linear solves converge; bitwise determinism; batch == alone.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_lib
+from primal_dual_contacts_miror_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+PARITY = 1e-9
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from primal_dual_contacts_miror_b200 import lib
+
+    return lib
+
+
+def rel(a, b, floor=1e-300):
+    """Normwise relative difference max|a-b| / max(max|b|, floor)."""
+    scale = max(np.abs(b).max() if b.size else 0.0, floor)
+    return np.abs(a - b).max() / scale if a.size else 0.0
+
+
+def compare(gpu_out, ora_out, tol=PARITY, iters=1, g=9.81, dt=0.01):
+    """Impulses relative to the largest impulse; velocity increments relative to
+    max(largest increment, |g| dt) -- a resting body's increment is pure solver
+    residual (~tol * charSpeed), so |g| dt is the physical velocity scale."""
+    dv, da, lf, st = gpu_out
+    odv, oda, olf, ost = ora_out
+    vel = np.concatenate([dv, da], 1)
+    ovel = np.concatenate([odv, oda], 1)
+    assert rel(lf, olf) < tol, ("impulse", rel(lf, olf), st, ost)
+    assert rel(vel, ovel, g * dt) < tol, ("velocity", rel(vel, ovel, g * dt), st, ost)
+    assert abs(st["newton_iters"] - ost["newton_iters"]) <= iters, (st, ost)
+
+
+CASES = {
+    "box_on_ground": lambda: (scenes.box_on_ground(), (0, 0, -9.81)),
+    "stack10": lambda: (scenes.resting_box_stack(10), (0, 0, -9.81)),
+    "incline30": lambda: (scenes.box_on_ground(), (9.81 * math.sin(math.radians(30)), 0, -9.81 * math.cos(math.radians(30)))),
+    "incline20": lambda: (scenes.box_on_ground(), (9.81 * math.sin(math.radians(20)), 0, -9.81 * math.cos(math.radians(20)))),
+    "sphere": lambda: (scenes.sliding_sphere(vel=(3, 0, 0)), (0, 0, -9.81)),
+    "columns": lambda: (scenes.box_columns(9, 4, seed=5, vel_noise=0.01, tilt=0.0), (0, 0, -9.81)),
+}
+
+
+# Scenes whose final state the reference algorithm itself only determines to
+# about the Newton tolerance: unloaded symmetric stacks sit at the apex of the
+# smoothed cone, where d(grad)/df_t ~ 1/sqrt(1e-16) amplifies round-off ~1e6x
+# per early iteration.  The oracle against itself (LDL^T vs CG branch, or a
+# permuted contact order) moves by up to ~100x tol there (test_oracle_envelope.py),
+# so the bar for them is that envelope, not 1e-9.
+ENVELOPE = {"stack10": 100.0}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_single_scene_parity(gpu, name, tol):
+    s, g = CASES[name]()
+    cfg = abi.default_config(tol=tol)
+    solver = gpu.Solver(cfg)
+    out = solver.solve(s, dt=0.01, gravity=g)
+    ora = oracle_lib.solve(s, dt=0.01, gravity=g, cfg=cfg)
+    bar = max(PARITY, ENVELOPE[name] * tol) if name in ENVELOPE else PARITY
+    compare(out, ora, tol=bar)
+
+
+def test_stack_resultants_match(gpu):
+    """Per-interface resultant impulses of the 10-box stack (well determined even
+    where individual corner impulses are not) agree with the oracle."""
+    s = scenes.resting_box_stack(10)
+    cfg = abi.default_config(tol=1e-8)
+    dv, da, lf, st = gpu.Solver(cfg).solve(s)
+    odv, oda, olf, ost = oracle_lib.solve(s, cfg=cfg)
+    res = lambda x: x.reshape(10, 4, 3).sum(1)
+    assert rel(res(lf), res(olf)) < 1e-7
+    assert rel(np.concatenate([dv, da], 1), np.concatenate([odv, oda], 1), 0.0981) < 1e-7
+
+
+def test_known_answers_on_gpu(gpu):
+    s = scenes.resting_box_stack(10)
+    solver = gpu.Solver(abi.default_config(tol=1e-8))
+    dv, da, lf, st = solver.solve(s)
+    fn = lf[:, 0].reshape(10, 4).sum(1) / (s.mass[1] * 9.81 * 0.01)
+    np.testing.assert_allclose(fn, np.arange(10, 0, -1), rtol=1e-6)
+    assert st["status"] == 0 and st["kkt_cone"] <= 0
+
+
+def test_deterministic_bitwise(gpu):
+    s = scenes.box_columns(16, 6, seed=11, vel_noise=0.01, tilt=0.01)
+    solver = gpu.Solver(abi.default_config(tol=1e-8))
+    a = solver.solve(s)
+    b = solver.solve(s)
+    for x, y in zip(a[:3], b[:3]):
+        assert np.array_equal(x, y)
+
+
+def test_batch_equals_alone_bitwise(gpu):
+    sc = [scenes.box_columns(k + 2, 3 + k % 3, seed=100 + k, vel_noise=0.01, tilt=0.01) for k in range(12)]
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    solver = gpu.Solver(abi.default_config(tol=1e-8))
+    dv, da, lf, st = solver.batch_solve(batch)
+    for k, s in enumerate(sc):
+        one = solver.solve(s)
+        b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
+        c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
+        assert np.array_equal(dv[b0:b1], one[0])
+        assert np.array_equal(lf[c0:c1], one[2])
+        assert st[k]["newton_iters"] == one[3]["newton_iters"]
+
+
+def test_batch_parity_with_oracle(gpu):
+    sc = [scenes.box_columns(k + 2, 3, seed=200 + k, vel_noise=0.01, tilt=0.0) for k in range(8)]
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    cfg = abi.default_config(tol=1e-8)
+    out = gpu.Solver(cfg).batch_solve(batch)
+    ora = oracle_lib.batch_solve(batch, cfg=cfg, scene_parallel=1, nthreads=4)
+    for k in range(len(sc)):
+        b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
+        c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
+        compare((out[0][b0:b1], out[1][b0:b1], out[2][c0:c1], out[3][k]),
+                (ora[0][b0:b1], ora[1][b0:b1], ora[2][c0:c1], ora[3][k]))
+
+
+def test_no_contacts(gpu):
+    s = scenes.box_on_ground()
+    s2 = abi.HostScene(s.vel, s.ang_vel, s.mass, s.inertia, s.inv_inertia, s.is_static,
+                       np.zeros((0, 2), np.int32), np.zeros((0, 9)), np.zeros((0, 6)))
+    dv, da, lf, st = gpu.Solver().solve(s2)
+    np.testing.assert_allclose(dv, np.tile([0, 0, -0.0981], (2, 1)))
+    assert st["newton_iters"] == 0
+
+
+def test_bad_body_id_is_einval(gpu):
+    s = scenes.box_on_ground()
+    body = s.body.copy()
+    body[0, 1] = 7
+    s2 = abi.HostScene(s.vel, s.ang_vel, s.mass, s.inertia, s.inv_inertia, s.is_static, body, s.frame, s.arm)
+    with pytest.raises(gpu.PdcError) as e:
+        gpu.Solver().solve(s2)
+    assert e.value.code == abi.PDC_EINVAL
+
+
+def test_iterative_branch_runs(gpu):
+    s = scenes.resting_box_stack(6)
+    cfg = abi.default_config(tol=1e-9, direct_threshold=1)
+    dv, da, lf, st = gpu.Solver(cfg).solve(s)
+    odv, oda, olf, ost = oracle_lib.solve(s, cfg=cfg)
+    assert st["pcg_iters"] > 0
+    assert rel(lf, olf) < 1e-6
