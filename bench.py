@@ -1,0 +1,291 @@
+"""Benchmark of the batched primal-dual contact solve on B200.
+
+Workload (one "step" = one solver pass over one batch): 4,096 independent
+box-pile contact problems with body counts log-uniform in [4, 256] (the
+batched workload's size distribution), FP64, Newton tolerance 1e-6, solved in
+one persistent launch (one CTA per scene, scenes handed out by an atomic work
+counter).  Inputs are seeded synthetic settled piles (scenes.pile_batch); the
+4,096-scene working set (~1.2 GB) is larger than L2, so no flush is needed
+between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own 4,096 scenes
+(scenes shard with no exchange: weak scaling); time = max over ranks.
+--impl reference times the reference algorithm's CPU implementation (the C++
+oracle restating it, OpenMP over all host cores) on a bounded sample.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from primal_dual_contacts_miror_b200 import abi, scenes  # noqa: E402
+
+METRIC = "scene-steps/s"
+SEED = 20241203 + 3 * 10 ** 6
+
+
+def algorithmic_bytes(stats, n_contacts):
+    """Bytes the solve must move per step, counted once per pass over each array
+    (FP64): contact geometry G=144, contact state S=40, contact scratch Q=88,
+    body record B=152, block preconditioner P=168, body vector V=48.  Passes:
+    residual  Nc(G+S)+Nb(B+V); assembly Nc(G+S+Q)+Nb(B-48+V+P);
+    PCG iter  Nc(G+32)+Nb(P+6V+56); recovery Nc(G+Q+56)+Nb V;
+    line-search trial Nc(G+2S)+Nb(3V+56); sparse direct solve 3 (blocks + Nb) 288."""
+    G, S, Q, B, P, V = 144, 40, 88, 152, 168, 48
+    total = 0.0
+    for st, nc in zip(stats, n_contacts):
+        nc = int(nc)
+        nb = int(st["n_local_bodies"])
+        it = st["newton_iters"]
+        ev = nc * (G + S) + nb * (B + V)
+        asm = nc * (G + S + Q) + nb * (B - 48 + V + P)
+        rec = nc * (G + Q + 56) + nb * V
+        pcg = nc * (G + 32) + nb * (P + 6 * V + 56)
+        ls = nc * (G + 2 * S) + nb * (3 * V + 56)
+        dense = 3 * (int(st["factor_blocks"]) + nb) * 36 * 8  # factor RMW + 2 triangular sweeps
+        total += (it + 1) * ev + it * (asm + rec + dense) + st["pcg_iters"] * pcg + st["ls_trials"] * ls
+    return total
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(n_scenes, seed):
+    sc = scenes.pile_batch(n_scenes, seed)
+    return abi.HostBatch(sc, 0.01, (0.0, 0.0, -9.81))
+
+
+def cpu_reference(batch, cfg, sample, nthreads):
+    """Time the CPU restatement (scene-parallel OpenMP) on the first `sample` scenes."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib  # the reference algorithm's CPU implementation (checker only)
+
+    sub = abi.HostBatch(batch.scenes[:sample], 0.01, (0.0, 0.0, -9.81))
+    t0 = time.perf_counter()
+    oracle_lib.batch_solve(sub, cfg=cfg, scene_parallel=1, nthreads=nthreads)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    batch = build_workload(args.scenes, SEED)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+
+    cores = oracle_lib.load().pdc_oracle_physical_processors()
+    sample = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_reference(batch, cfg, min(sample, 16), cores)
+    times = [cpu_reference(batch, cfg, sample, cores) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    value = sample / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 * args.scenes / sample,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.scenes} box-pile scenes, 4-256 bodies log-uniform, tol {cfg.tol}",
+                   "sample_scenes": sample, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"first {sample} of {args.scenes} scenes per step, scene-parallel OpenMP"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenes", type=int, default=4096)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--sparse-max", type=int, default=256)
+    ap.add_argument("--warp-max-contacts", type=int, default=4096)
+    ap.add_argument("--warp-max-bodies", type=int, default=512)
+    ap.add_argument("--cpu-sample", type=int, default=512)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    cfg = abi.default_config(tol=args.tol, sparse_max_bodies=args.sparse_max,
+                             warp_max_contacts=args.warp_max_contacts, warp_max_bodies=args.warp_max_bodies)
+    if args.impl == "reference":
+        run_reference(args, cfg)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from primal_dual_contacts_miror_b200 import lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg.device = local
+    solver = lib.Solver(cfg)
+    batch = build_workload(args.scenes, SEED + 7919 * rank)
+    dev = lib.DeviceBatch(batch, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        solver.batch_solve_device(dev, sh)
+    torch.cuda.synchronize()
+    stats = dev.stats_list()
+    n_contacts = np.diff(batch.contact_offsets)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        solver.batch_solve_device(dev, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    per_step_s = ms_max / 1e3 / args.steps
+    value = args.scenes * world / per_step_s
+    newton = sum(s["newton_iters"] for s in stats)
+    ci = float(np.sum(n_contacts * np.array([s["newton_iters"] for s in stats])))
+
+    # end to end through the public C ABI with host arrays (H2D + D2H per step)
+    a = batch.all
+    h2d = sum(x.nbytes for x in (a.vel, a.ang_vel, a.mass, a.inertia, a.inv_inertia, a.is_static, a.body, a.frame,
+                                 a.arm, a.depth, batch.body_offsets, batch.contact_offsets, batch.dt, batch.gravity))
+    d2h = (a.n_bodies * 6 + a.n_contacts * 3) * 8 + batch.n_scenes * C.sizeof(abi.Stats)
+    e2e_steps = max(1, min(args.steps, 5))
+    solver.batch_solve(batch)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.batch_solve(batch)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    et = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = args.scenes * world / float(et.item())
+
+    peak, peak_kind = load_peaks()
+    ab = algorithmic_bytes(stats, n_contacts)
+    achieved = ab / per_step_s / 1e9
+    status_counts = {}
+    for s in stats:
+        status_counts[str(s["status"])] = status_counts.get(str(s["status"]), 0) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.scenes} box-pile scenes per GPU, 4-256 bodies log-uniform, plain FP64, "
+                               f"tol {args.tol}, one persistent launch per step",
+                   "contacts_per_gpu": int(a.n_contacts), "bodies_per_gpu": int(a.n_bodies),
+                   "sparse_max_bodies": args.sparse_max, "warp_max_contacts": args.warp_max_contacts,
+                   "warp_max_bodies": args.warp_max_bodies, "l2": "inputs larger than L2 (no flush)"},
+        "contact_newton_iters_per_s": ci * world / per_step_s,
+        "newton_iters_mean": newton / len(stats),
+        "scene_status": status_counts,
+        "gpu_launches": 2 * args.steps,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": ab, "kernel": "solve_scenes_kernel"},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+
+        cores = oracle_lib.load().pdc_oracle_physical_processors()
+        tc = cpu_reference(batch, cfg, args.cpu_sample, cores)
+        line["cpu_baseline"] = {"value": args.cpu_sample / tc, "unit": METRIC, "cores": cores, "kind": "port",
+                                "sample": f"first {args.cpu_sample} of {args.scenes} scenes, one pass, "
+                                          f"scene-parallel OpenMP"}
+    if rank == 0:
+        print(json.dumps(line))
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -88,8 +88,12 @@ typedef struct pdc_config {
     double spring_damp;       /* non_smooth_force.spring_damp (0.01) */
     int32_t precision;        /* enum pdc_precision */
     int32_t direct_threshold; /* local bodies below this use the direct-solve branch (2000) */
-    int32_t dense_max_bodies; /* direct branch: dense Cholesky on the device up to this many
-                                 active bodies (64); larger scenes use PCG */
+    int32_t sparse_max_bodies; /* direct branch: sparse block Cholesky on the device up to
+                                  this many active bodies (256, the maximum); larger
+                                  scenes use PCG */
+    int32_t warp_max_contacts; /* batched launch: scenes with at most this many contacts */
+    int32_t warp_max_bodies;   /* and bodies are solved by one warp, larger ones by a
+                                  whole thread block (4096 / 512; 0 = blocks only) */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
     int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
     double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */
@@ -128,6 +132,8 @@ typedef struct pdc_stats {
     int32_t ls_trials;      /* total line-search trials */
     int32_t gd_fallbacks;   /* gradient-descent fallbacks (:444-467) */
     int32_t n_local_bodies; /* bodies in contact (:96-111) */
+    int32_t factor_blocks;  /* off-diagonal 6x6 blocks of the sparse factor (0: PCG) */
+    int32_t team;           /* 0: solved by a thread block, 1: by one warp */
     double exit_err;        /* exitErr at exit (:302-307) */
     double kkt_stationarity;/* max(|ru|/6N_b, |rf|/3N_c) */
     double kkt_complementarity; /* max(|lambda.c|_inf, dual gap) */
@@ -166,8 +172,9 @@ int pdc_solve(pdc_solver* s, double dt, const double gravity[3],
               pdc_result* out);
 
 /* Same as pdc_solve but every pointer in bodies/contacts/out is a DEVICE pointer
- * and the work is enqueued on `stream` (a cudaStream_t; NULL = legacy stream).
- * out->stats is filled when the stream is synchronized via pdc_sync. */
+ * (is_static and depth required) and the work is enqueued on `stream` (a
+ * cudaStream_t; NULL = legacy default stream).  out->stats is zeroed, not
+ * filled: per-scene statistics come from pdc_batch_solve_async. */
 int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3],
                     const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
                     pdc_result* out, void* stream);
@@ -191,8 +198,10 @@ int pdc_batch_solve(pdc_solver* s, const pdc_batch* batch,
                     double* dvel, double* dang_vel, double* local_force,
                     pdc_stats* stats);
 
-/* Device arrays (batch offsets/dt/gravity too); enqueued on `stream`.
- * stats (device, n_scenes entries) may be NULL. */
+/* Device arrays (batch offsets/dt/gravity too); enqueued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  The caller synchronizes that
+ * stream; calls on one handle must not overlap in time (they share its
+ * workspace).  stats (device, n_scenes entries) may be NULL. */
 int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
                           const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
                           double* dvel, double* dang_vel, double* local_force,

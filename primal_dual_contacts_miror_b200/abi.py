@@ -42,7 +42,9 @@ class Config(C.Structure):
         ("spring_damp", C.c_double),
         ("precision", C.c_int32),
         ("direct_threshold", C.c_int32),
-        ("dense_max_bodies", C.c_int32),
+        ("sparse_max_bodies", C.c_int32),
+        ("warp_max_contacts", C.c_int32),
+        ("warp_max_bodies", C.c_int32),
         ("pcg_rtol_direct", C.c_double),
         ("pcg_max_direct", C.c_int32),
         ("pcg_rtol_iter", C.c_double),
@@ -84,6 +86,8 @@ class Stats(C.Structure):
         ("ls_trials", C.c_int32),
         ("gd_fallbacks", C.c_int32),
         ("n_local_bodies", C.c_int32),
+        ("factor_blocks", C.c_int32),
+        ("team", C.c_int32),
         ("exit_err", C.c_double),
         ("kkt_stationarity", C.c_double),
         ("kkt_complementarity", C.c_double),
@@ -130,7 +134,9 @@ def default_config(**overrides):
     cfg.spring_damp = 0.01
     cfg.precision = PDC_PRECISION_FP64
     cfg.direct_threshold = 2000
-    cfg.dense_max_bodies = 64
+    cfg.sparse_max_bodies = 256
+    cfg.warp_max_contacts = 4096
+    cfg.warp_max_bodies = 512
     cfg.pcg_rtol_direct = 1e-13
     cfg.pcg_max_direct = 4000
     cfg.pcg_rtol_iter = 1e-8

@@ -20,6 +20,11 @@
 namespace {
 
 thread_local std::string g_create_error;
+constexpr int kThreads = 256;
+constexpr int kWarpsPerBlock = kThreads / 32;
+// sparse scratch: bitsets, orders, offsets, 2x256 diagonal blocks, 3 node vectors
+constexpr long long kSparseHeaderDoubles = 30720;
+constexpr long long kSparseBlocks = 3072;  // off-diagonal L blocks per scene
 
 struct Arena {
     void* base = nullptr;
@@ -78,7 +83,9 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.spring_k = c.spring_k;
     e.spring_damp = c.spring_damp;
     e.direct_threshold = c.direct_threshold;
-    e.dense_max = c.dense_max_bodies;
+    e.dense_max = c.sparse_max_bodies;
+    e.warp_max_contacts = c.warp_max_contacts;
+    e.warp_max_bodies = c.warp_max_bodies;
     e.rtol_direct = c.pcg_rtol_direct;
     e.max_direct = c.pcg_max_direct;
     e.rtol_iter = c.pcg_rtol_iter;
@@ -97,7 +104,6 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
         P->contact_off = I(ns + 1);
         P->dt = D(ns);
         P->grav = D(3 * ns);
-        P->order = I(ns);
         P->vel = D(3 * nb);
         P->ang = D(3 * nb);
         P->mass = D(nb);
@@ -148,10 +154,13 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->W = D(6 * nc);
     P->didx = I(nb);
     P->dbody = I(nb);
+    P->order_cta = I(ns);
+    P->order_warp = I(ns);
+    P->counts = I(4);
     if (dense_max > 0) {
-        const long long NM = 6LL * dense_max;
-        P->dense_stride = NM * NM + 3 * NM;
-        P->dense = D((size_t)grid * P->dense_stride);
+        // sparse factorisation scratch per team: fixed header + L blocks
+        P->dense_stride = kSparseHeaderDoubles + 36LL * kSparseBlocks;
+        P->dense = D((size_t)grid * (1 + kWarpsPerBlock) * P->dense_stride);
     } else {
         P->dense = nullptr;
         P->dense_stride = 0;
@@ -163,7 +172,7 @@ static int grid_for(const pdc_solver* s, int ns) { return std::max(1, std::min(n
 
 static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::BatchPtrs* P, bool host_inputs) {
     const int grid = grid_for(s, ns);
-    const int dmax = s->cfg.dense_max_bodies;
+    const int dmax = s->cfg.sparse_max_bodies;
     Arena probe;
     probe.base = nullptr;
     size_t need = carve(probe, ns, nb, nc, P, host_inputs, grid, dmax);
@@ -197,7 +206,9 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->spring_damp = 0.01;
     c->precision = PDC_PRECISION_FP64;
     c->direct_threshold = 2000;  // :385
-    c->dense_max_bodies = 64;
+    c->sparse_max_bodies = 256;
+    c->warp_max_contacts = 4096;
+    c->warp_max_bodies = 512;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;
     c->pcg_rtol_iter = 1e-8;
@@ -216,7 +227,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
     if (c->precision != PDC_PRECISION_FP64 && c->precision != PDC_PRECISION_MIXED)
         return fail(s, PDC_EINVAL, "unknown precision");
     if (c->pcg_max_direct <= 0 || c->pcg_max_iter <= 0) return fail(s, PDC_EINVAL, "bad PCG caps");
-    if (c->dense_max_bodies < 0 || c->dense_max_bodies > 256) return fail(s, PDC_EINVAL, "dense_max_bodies out of [0, 256]");
+    if (c->sparse_max_bodies < 0 || c->sparse_max_bodies > pdc::kSparseMax)
+        return fail(s, PDC_EINVAL, "sparse_max_bodies out of [0, 256]");
     return PDC_OK;
 }
 
@@ -239,7 +251,7 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel, 256, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel, kThreads, 0);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_timers, 4 * sizeof(unsigned long long) + 16);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_counter, 16);
     if (e == cudaSuccess) e = cudaMemset(s->d_timers, 0, 4 * sizeof(unsigned long long));
@@ -278,13 +290,13 @@ extern "C" int pdc_reset(pdc_solver* s) {
 
 static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st) {
     pdc::BatchPtrs P = P0;
-    P.work_counter = s->d_counter;
     P.timers = s->d_timers;
-    CK(cudaMemsetAsync(s->d_counter, 0, sizeof(int), st), "memset counter");
     if (P.n_scenes == 0) return PDC_OK;
     const int grid = grid_for(s, P.n_scenes);
     pdc::EngineCfg C = engine_cfg(s->cfg);
-    pdc::solve_scenes_kernel<<<grid, 256, 0, st>>>(P, C);
+    pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
+    CK(cudaGetLastError(), "launch plan_scenes_kernel");
+    pdc::solve_scenes_kernel<<<grid, kThreads, 0, st>>>(P, C);
     CK(cudaGetLastError(), "launch solve_scenes_kernel");
     return PDC_OK;
 }
@@ -331,13 +343,6 @@ static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_so
     if (rc) return rc;
     P.n_scenes = ns;
     cudaStream_t st = s->stream;
-    // largest scenes first for load balance across CTAs
-    std::vector<int> order(ns);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return (batch->contact_offsets[x + 1] - batch->contact_offsets[x]) >
-               (batch->contact_offsets[y + 1] - batch->contact_offsets[y]);
-    });
     std::vector<double> mu_fill;
     auto H2D = [&](const void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice, st);
@@ -346,7 +351,6 @@ static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_so
     CK(H2D(P.contact_off, batch->contact_offsets, (ns + 1) * sizeof(int)), "H2D");
     CK(H2D(P.dt, batch->dt, ns * sizeof(double)), "H2D");
     CK(H2D(P.grav, batch->gravity, 3 * ns * sizeof(double)), "H2D");
-    CK(H2D(P.order, order.data(), ns * sizeof(int)), "H2D");
     if (nb) {
         CK(H2D(P.vel, b->vel, 3 * nb * sizeof(double)), "H2D");
         CK(H2D(P.ang, b->ang_vel, 3 * nb * sizeof(double)), "H2D");
@@ -423,7 +427,6 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
     P.contact_off = batch->contact_offsets;
     P.dt = batch->dt;
     P.grav = batch->gravity;
-    P.order = nullptr;
     P.vel = b->vel;
     P.ang = b->ang_vel;
     P.mass = b->mass;
@@ -440,7 +443,8 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
     P.lforce = local_force;
     P.stats = stats;
     if (!P.is_static || !P.depth) return fail(s, PDC_EINVAL, "device path needs is_static and depth arrays");
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    // NULL is the legacy default stream, as for every CUDA runtime call
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     rc = launch(s, P, st);
     if (rc) return rc;
     s->solves += batch->n_scenes;
@@ -449,13 +453,42 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
 
 extern "C" int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3], const pdc_bodies_soa* bodies,
                                const pdc_contacts_soa* contacts, pdc_result* out, void* stream) {
-    (void)dt;
-    (void)gravity;
-    (void)bodies;
-    (void)contacts;
-    (void)out;
-    (void)stream;
-    return fail(s, PDC_EINVAL, "pdc_solve_async: use pdc_batch_solve_async with one scene");
+    if (!s) return PDC_EINVAL;
+    if (!gravity || !bodies || !contacts || !out || !out->dvel || !out->dang_vel || !out->local_force)
+        return fail(s, PDC_EINVAL, "null argument");
+    if (bodies->n < 0 || contacts->n < 0 || !(dt > 0)) return fail(s, PDC_EINVAL, "bad size or time step");
+    if (!bodies->is_static || !contacts->depth) return fail(s, PDC_EINVAL, "device path needs is_static and depth");
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    pdc::BatchPtrs P;
+    std::memset(&P, 0, sizeof(P));
+    int rc = ensure_arena(s, 1, std::max(bodies->n, 1), std::max(contacts->n, 1), &P, false);
+    if (rc) return rc;
+    P.n_scenes = 1;
+    P.body_off = nullptr;  // single-scene launch: sizes by value
+    P.single_nb = bodies->n;
+    P.single_nc = contacts->n;
+    P.single_dt = dt;
+    for (int k = 0; k < 3; ++k) P.single_g[k] = gravity[k];
+    P.vel = bodies->vel;
+    P.ang = bodies->ang_vel;
+    P.mass = bodies->mass;
+    P.inertia = bodies->inertia;
+    P.inv_inertia = bodies->inv_inertia;
+    P.is_static = bodies->is_static;
+    P.cbody = contacts->body;
+    P.frame = contacts->frame;
+    P.arm = contacts->arm;
+    P.depth = contacts->depth;
+    P.cmu = contacts->mu;
+    P.dvel = out->dvel;
+    P.dang = out->dang_vel;
+    P.lforce = out->local_force;
+    P.stats = nullptr;  // per-scene statistics: use pdc_batch_solve_async
+    std::memset(&out->stats, 0, sizeof(out->stats));
+    rc = launch(s, P, static_cast<cudaStream_t>(stream));
+    if (rc) return rc;
+    s->solves += 1;
+    return PDC_OK;
 }
 
 extern "C" int pdc_sync(pdc_solver* s, int32_t timeout_ms) {

@@ -123,6 +123,112 @@ struct BlockReducer {
     }
 };
 
+// ------------------------------------------------------------------ teams
+// A team is the group of threads that solves one scene: a whole CTA (large
+// scenes; __syncthreads, shared-memory reductions) or one warp (small scenes;
+// __syncwarp and shuffles only, so a block hosts many independent scenes).
+// Both give every member the bitwise-identical result of each reduction.
+struct CtaTeam {
+    int rank, size, slot;
+    BlockReducer<8> red;
+    int* s_int;  // shared: [0] carry, [1..32] warp partials
+    __device__ CtaTeam(double* red_smem, int* int_smem) {
+        rank = threadIdx.x;
+        size = blockDim.x;
+        slot = blockIdx.x;
+        red.init(red_smem);
+        s_int = int_smem;
+    }
+    __device__ __forceinline__ void sync() { __syncthreads(); }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) { red.sum(v); }
+    template <int N>
+    __device__ __forceinline__ void max(double (&v)[N]) { red.max(v); }
+    // exclusive scan over n items: put(i, carry0 + prefix)
+    template <typename Get, typename Put>
+    __device__ void scan(int n, int carry0, Get get, Put put) {
+        int* s_carry = s_int;
+        int* s_warp = s_int + 1;
+        if (rank == 0) *s_carry = carry0;
+        __syncthreads();
+        const int lane = rank & 31, warp = rank >> 5;
+        for (int base = 0; base < n; base += size) {
+            const int b = base + rank;
+            const int val = (b < n) ? get(b) : 0;
+            int x = val;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_warp[warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                int w = (lane < (size >> 5)) ? s_warp[lane] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                s_warp[lane] = w;
+            }
+            __syncthreads();
+            const int excl = x - val + (warp ? s_warp[warp - 1] : 0) + *s_carry;
+            if (b < n) put(b, excl);
+            __syncthreads();
+            if (rank == size - 1) *s_carry = excl + val;
+            __syncthreads();
+        }
+    }
+};
+
+struct WarpTeam {
+    int rank, size, slot;
+    __device__ WarpTeam(int slot_) {
+        rank = threadIdx.x & 31;
+        size = 32;
+        slot = slot_;
+    }
+    __device__ __forceinline__ void sync() { __syncwarp(); }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            v[i] = __shfl_sync(0xffffffffu, x, 0);
+        }
+    }
+    template <int N>
+    __device__ __forceinline__ void max(double (&v)[N]) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_down_sync(0xffffffffu, x, o));
+            v[i] = __shfl_sync(0xffffffffu, x, 0);
+        }
+    }
+    template <typename Get, typename Put>
+    __device__ void scan(int n, int carry0, Get get, Put put) {
+        int carry = carry0;
+        for (int base = 0; base < n; base += 32) {
+            const int b = base + rank;
+            const int val = (b < n) ? get(b) : 0;
+            int x = val;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (rank >= o) x += y;
+            }
+            if (b < n) put(b, carry + x - val);
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        __syncwarp();
+    }
+};
+
 // 6x6 symmetric positive definite inverse via Cholesky; input/output packed
 // lower triangle, row-major (21 values: (0,0),(1,0),(1,1),(2,0),...).
 __device__ __forceinline__ int pk(int r, int c) { return (r >= c) ? (r * (r + 1) / 2 + c) : (c * (c + 1) / 2 + r); }

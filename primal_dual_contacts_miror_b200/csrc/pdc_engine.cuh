@@ -33,7 +33,9 @@ struct EngineCfg {
     double compliance_coef;  // m_compliance numerator inputs
     double spring_k, spring_damp;
     int direct_threshold;
-    int dense_max;  // direct branch: dense Cholesky up to this many active bodies
+    int dense_max;  // direct branch: sparse Cholesky up to this many active bodies (<= kSparseMax)
+    int warp_max_contacts;  // scenes up to this size are solved by one warp
+    int warp_max_bodies;
     double rtol_direct;
     int max_direct;
     double rtol_iter;
@@ -42,11 +44,13 @@ struct EngineCfg {
 
 struct BatchPtrs {
     int n_scenes;
+    // single-scene launch (body_off == nullptr): sizes and step passed by value
+    int single_nb, single_nc;
+    double single_dt, single_g[3];
     const int* __restrict__ body_off;
     const int* __restrict__ contact_off;
     const double* __restrict__ dt;
     const double* __restrict__ grav;
-    const int* __restrict__ order;  // optional scene order (may be null)
     // bodies (inputs)
     const double* __restrict__ vel;
     const double* __restrict__ ang;
@@ -101,14 +105,21 @@ struct BatchPtrs {
     double* W;      // 6 R K^-1 R^T packed (xx,yy,zz,xy,xz,yz)
     int* didx;   // dense row-block of each active body
     int* dbody;  // body of each dense row-block (scene-relative slots)
-    // per-CTA dense scratch: (6 dense_max)^2 matrix + 3 vectors of 6 dense_max
+    // per-team sparse-factorisation scratch (see SceneSolver::sparse_ws)
     double* dense;
     long long dense_stride;
-    int* work_counter;
+    int* order_cta;   // scene queues written by plan_scenes_kernel
+    int* order_warp;
+    int* counts;      // [4]
     unsigned long long* timers;  // [4] ns: total, build, solve, line search
 };
 
 #define PDC_STATUS_BAD_INPUT 16
+
+// sparse direct solve: nodes per scene (bitset width) 
+constexpr int kSparseMax = 256;
+constexpr int kSparseWords = kSparseMax / 32;
+constexpr int kRowCap = 3072;  // off-diagonal factor blocks per scene
 
 // W = R diag(kn, Kt^-1) R^T (packed symmetric)
 __device__ __forceinline__ void frame_sandwich(const Frame& R, double kni, double t00, double t01, double t11,
@@ -139,11 +150,12 @@ __device__ __forceinline__ d3 point_vel(const double* u6, d3 c) {
     return add3(v, cross3(w, c));
 }
 
+template <class Team>
 class SceneSolver {
    public:
     const BatchPtrs& B;
     const EngineCfg& C;
-    BlockReducer<8>& red;
+    Team& T;
     int s, b0, nb, c0, nc, tid, nt;
     double dt, g[3];
     double cm, cs;  // charMass, charSpeed
@@ -153,18 +165,29 @@ class SceneSolver {
     int status;
     unsigned long long t_build, t_solve, t_ls, t_mark;
 
-    __device__ SceneSolver(const BatchPtrs& b, const EngineCfg& c, BlockReducer<8>& r, int scene)
-        : B(b), C(c), red(r), s(scene) {
-        b0 = B.body_off[s];
-        nb = B.body_off[s + 1] - b0;
-        c0 = B.contact_off[s];
-        nc = B.contact_off[s + 1] - c0;
-        tid = threadIdx.x;
-        nt = blockDim.x;
-        dt = B.dt[s];
-        g[0] = B.grav[3 * s];
-        g[1] = B.grav[3 * s + 1];
-        g[2] = B.grav[3 * s + 2];
+    __device__ SceneSolver(const BatchPtrs& b, const EngineCfg& c, Team& t, int scene)
+        : B(b), C(c), T(t), s(scene) {
+        if (B.body_off) {
+            b0 = B.body_off[s];
+            nb = B.body_off[s + 1] - b0;
+            c0 = B.contact_off[s];
+            nc = B.contact_off[s + 1] - c0;
+            dt = B.dt[s];
+            g[0] = B.grav[3 * s];
+            g[1] = B.grav[3 * s + 1];
+            g[2] = B.grav[3 * s + 2];
+        } else {
+            b0 = 0;
+            nb = B.single_nb;
+            c0 = 0;
+            nc = B.single_nc;
+            dt = B.single_dt;
+            g[0] = B.single_g[0];
+            g[1] = B.single_g[1];
+            g[2] = B.single_g[2];
+        }
+        tid = T.rank;
+        nt = T.size;
         status = 0;
         t_build = t_solve = t_ls = 0;
     }
@@ -206,43 +229,6 @@ class SceneSolver {
         y[5] = Ixz * v[3] + Iyz * v[4] + Izz * v[5];
     }
 
-    // Block-wide exclusive scan over the scene's bodies: put(b, carry0 + prefix).
-    template <typename Get, typename Put>
-    __device__ void block_scan(int carry0, Get get, Put put) {
-        __shared__ int s_carry;
-        __shared__ int s_warp[32];
-        if (tid == 0) s_carry = carry0;
-        __syncthreads();
-        for (int base = 0; base < nb; base += nt) {
-            const int b = base + tid;
-            const int val = (b < nb) ? get(b) : 0;
-            int x = val;
-            const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (lane == 31) s_warp[warp] = x;
-            __syncthreads();
-            if (warp == 0) {
-                int w = (lane < (nt >> 5)) ? s_warp[lane] : 0;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    int y = __shfl_up_sync(0xffffffffu, w, o);
-                    if (lane >= o) w += y;
-                }
-                s_warp[lane] = w;
-            }
-            __syncthreads();
-            const int excl = x - val + (warp ? s_warp[warp - 1] : 0) + s_carry;
-            if (b < nb) put(b, excl);
-            __syncthreads();
-            if (tid == nt - 1) s_carry = excl + val;
-            __syncthreads();
-        }
-    }
-
     // ------------------------------------------------------------ set-up
     // Returns false if the scene has no contacts (outputs already written).
     __device__ bool setup() {
@@ -259,7 +245,7 @@ class SceneSolver {
             B.local[gb] = 0;
         }
         if (nc == 0) return false;
-        __syncthreads();
+        T.sync();
         // count incidences, mark local bodies (renumbering :95-118)
         int bad = 0;
         for (int c = tid; c < nc; c += nt) {
@@ -272,10 +258,10 @@ class SceneSolver {
             }
         }
         double v[8] = {(double)bad, 0, 0, 0, 0, 0, 0, 0};
-        red.max(v);
+        T.max(v);
         if (v[0] > 0) { status |= PDC_STATUS_BAD_INPUT; return false; }
         // exclusive scan of counts -> absolute start in inc[]
-        block_scan(2 * c0, [&](int b) { return B.inc_cnt[b0 + b]; },
+        T.scan(nb, 2 * c0, [&](int b) { return B.inc_cnt[b0 + b]; },
                    [&](int b, int excl) { B.inc_start[b0 + b] = excl; });
         // fill incidence lists (slot order arbitrary, sorted below)
         for (int c = tid; c < nc; c += nt) {
@@ -318,7 +304,7 @@ class SceneSolver {
                 B.X[3 * gc + j] = sp;
             }
         }
-        __syncthreads();
+        T.sync();
         // sort incidence lists, per-body speed, mass sums
         double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // n_local, n_active, traceSum, m*speed, m
         for (int b = tid; b < nb; b += nt) {
@@ -348,7 +334,7 @@ class SceneSolver {
             acc[3] += spd * m;
             acc[4] += m;
         }
-        red.sum(acc);
+        T.sum(acc);
         n_local = (int)acc[0];
         n_active = (int)acc[1];
         cm = (n_active > 0) ? acc[2] / n_active / 6 : 1;  // :36
@@ -357,17 +343,19 @@ class SceneSolver {
         csv = dmax(csv, gn * dt * 0.25);
         csv = dmax(csv, 1e-4);
         cs = csv;
-        // dense direct solve for small scenes on the direct branch (LDLT analogue)
+        // sparse direct solve for scenes on the direct branch (the SimplicialLDLT
+        // analogue, :385-394): compact node numbering + symbolic factorisation
         dense_mode = B.dense != nullptr && n_local < C.direct_threshold && C.dense_max > 0 &&
-                     n_active <= C.dense_max && n_active > 0;
+                     n_active <= C.dense_max && n_active > 0 && C.dense_max <= kSparseMax;
         if (dense_mode) {
-            block_scan(0, [&](int b) { return active(b0 + b) ? 1 : 0; },
-                       [&](int b, int excl) {
-                           if (active(b0 + b)) {
-                               B.didx[b0 + b] = excl;
-                               B.dbody[b0 + excl] = b0 + b;
-                           }
-                       });
+            T.scan(nb, 0, [&](int b) { return active(b0 + b) ? 1 : 0; },
+                   [&](int b, int excl) {
+                       if (active(b0 + b)) {
+                           B.didx[b0 + b] = excl;
+                           B.dbody[b0 + excl] = b0 + b;
+                       }
+                   });
+            dense_mode = sparse_symbolic();
         }
         // velocities (non-dimensional) :203-217
         for (int b = tid; b < nb; b += nt) {
@@ -391,7 +379,7 @@ class SceneSolver {
         compliance = 1. / (dt * (tk + damp));
         reduction = tk / (tk + damp);
         spring_term = (C.spring_based ? 1.0 : 0.0) * compliance * cm;
-        __syncthreads();
+        T.sync();
         for (int c = tid; c < nc; c += nt) {
             const int gc = c0 + c;
             double k = 0;
@@ -408,7 +396,7 @@ class SceneSolver {
             B.lam[2 * gc] = 1e-2;
             B.lam[2 * gc + 1] = 1e-2;
         }
-        __syncthreads();
+        T.sync();
         return true;
     }
 
@@ -528,7 +516,7 @@ class SceneSolver {
                 B.hs[3 * gc + 2] = h2;
                 acc[0] += B.lam[2 * gc] * cn + B.lam[2 * gc + 1] * cc;
             }
-            red.sum(acc);
+            T.sum(acc);
             const double sDualGap = -(acc[0] / n_cons);
             const double muc = sDualGap * 0.1;
             // residuals at the current iterate (:292-300)
@@ -538,7 +526,7 @@ class SceneSolver {
                 contact_residual(gc, B.u, B.f + 3 * gc, B.lam + 2 * gc, true, muc, B.rf + 3 * gc, B.rl + 2 * gc,
                                  e[1], e[2], e[3]);
             }
-            __syncthreads();
+            T.sync();
             for (int b = tid; b < nb; b += nt) {
                 const int gb = b0 + b;
                 if (!B.local[gb]) continue;
@@ -548,7 +536,7 @@ class SceneSolver {
                 }
                 body_residual(gb, B.u + 6 * gb, B.ru + 6 * gb, e[0]);
             }
-            red.sum(e);
+            T.sum(e);
             const double err = e[0] + e[1] + e[2];
             const double sErr = err, sacErr = e[0] + e[3] + e[2];
             const double eps = Hu * pow(err, power * 0.5);
@@ -593,7 +581,7 @@ class SceneSolver {
                 const d3 ks = d3{sf0 * kni, t00 * sf1 + t01 * sf2, t01 * sf1 + t11 * sf2};
                 st3(B.X + 3 * gc, from_frame(R, ks));
             }
-            __syncthreads();
+            T.sync();
             // rhs = sum getTrans(j) K^-1 sf - ru; block-Jacobi blocks; PCG start
             double rr[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // r.z, b.b
             for (int b = tid; b < nb; b += nt) {
@@ -651,7 +639,7 @@ class SceneSolver {
                 }
                 for (int r = 0; r < 6; ++r) rr[1] += rb[r] * rb[r];
             }
-            red.sum(rr);  // sync: rhs, pinv complete
+            T.sum(rr);  // sync: rhs, pinv complete
             const double bnorm = sqrt(rr[1]);
             unsigned long long t1 = now();
             t_build += t1 - t_mark;
@@ -667,7 +655,7 @@ class SceneSolver {
             } else {
             if (!direct) {  // AMGCL starts from the previous du (:406-415)
                 spmv_to_X(B.du, nullptr, 0.0);
-                __syncthreads();
+                T.sync();
             }
             double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             for (int b = tid; b < nb; b += nt) {
@@ -691,7 +679,7 @@ class SceneSolver {
                     s2[1] += r6[r] * r6[r];
                 }
             }
-            red.sum(s2);
+            T.sum(s2);
             double rz = s2[0];
             double res = (bnorm > 0) ? sqrt(s2[1]) / bnorm : 0.0;
             double beta = 0;
@@ -701,7 +689,7 @@ class SceneSolver {
                 for (iters = 0; iters < maxit;) {
                     // contact phase: p_new = z + beta p for both bodies; X = W dv(p_new)
                     spmv_to_X(B.p, B.z, beta);
-                    __syncthreads();
+                    T.sync();
                     double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                     for (int b = tid; b < nb; b += nt) {
                         const int gb = b0 + b;
@@ -717,7 +705,7 @@ class SceneSolver {
                             B.z[6 * gb + r] = q6[r];  // z holds q until the update below
                         }
                     }
-                    red.sum(s3);
+                    T.sum(s3);
                     const double alpha = rz / s3[0];
                     double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                     for (int b = tid; b < nb; b += nt) {
@@ -736,7 +724,7 @@ class SceneSolver {
                             s4[1] += r6[r] * z6[r];
                         }
                     }
-                    red.sum(s4);
+                    T.sum(s4);
                     ++iters;
                     res = sqrt(s4[0]) / bnorm;
                     if (!(res >= rtol)) break;  // converged or non-finite
@@ -754,7 +742,7 @@ class SceneSolver {
                     for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = 0;
                 }
             }
-            __syncthreads();
+            T.sync();
             // retrieveNonSmoothForceInc (:254-280)
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
@@ -770,7 +758,7 @@ class SceneSolver {
                 B.dl[2 * gc + 1] = -B.invC[2 * gc + 1] *
                                    (B.lam[2 * gc + 1] * (B.gr[2 * gc] * e1 + B.gr[2 * gc + 1] * e2) + B.rl[2 * gc + 1]);
             }
-            __syncthreads();
+            T.sync();
             t1 = now();
             t_solve += t1 - t_mark;
             t_mark = t1;
@@ -794,7 +782,7 @@ class SceneSolver {
                     B.dl[2 * gc] = B.rl[2 * gc];
                     B.dl[2 * gc + 1] = B.rl[2 * gc + 1];
                 }
-                __syncthreads();
+                T.sync();
                 step = line_search(sErr, sacErr, muc, 20, trials);
                 ls_total += trials;
                 if (step == 0) ls_fail = true;
@@ -822,109 +810,422 @@ class SceneSolver {
         status = stt;
     }
 
-    // ---------------------------------------------- dense direct solve (small scenes)
-    __device__ __forceinline__ double* dense_A() const { return B.dense + (long long)blockIdx.x * B.dense_stride; }
+    // ------------------------------------------- sparse direct solve (direct branch)
+    // Per-team scratch: bitset adjacency / column patterns, elimination order,
+    // block-column offsets, diagonal blocks, their Cholesky factors, the L blocks
+    // and three node vectors.  Node i is the i-th active body of the scene.
+    struct Sparse {
+        uint32_t* adj;   // [kSparseMax][kSparseWords]
+        int* perm;       // elimination position -> node
+        int* ipos;       // node -> elimination position
+        int* cstart;     // [kSparseMax + 1] first L block of each node's column
+        int* lvl_nodes;  // nodes grouped by elimination-tree height
+        int* height;     // [kSparseMax] elimination-tree height of each node
+        int* lvl_start;  // [levels + 1]
+        int* rowptr;     // [kSparseMax + 1] row lists: columns d with L(v, d) != 0
+        int* rowidx;     // [kRowCap]
+        int* meta;       // [0] number of levels
+        double* Dg;      // [kSparseMax][36] diagonal blocks
+        double* Ld;      // [kSparseMax][36] Cholesky factor of each diagonal block
+        double* Ldi;     // [kSparseMax][6] reciprocal of the factor's diagonal
+        double* y;       // [kSparseMax][6]
+        double* z;       // [kSparseMax][6]
+        double* x;       // [kSparseMax][6]
+        double* L;       // [cap][36] off-diagonal blocks, column by column
+        int cap;
+    };
+    __device__ __forceinline__ Sparse sparse_ws() const {
+        char* p = reinterpret_cast<char*>(B.dense + (long long)T.slot * B.dense_stride);
+        Sparse S;
+        S.adj = reinterpret_cast<uint32_t*>(p);
+        p += kSparseMax * kSparseWords * 4;
+        S.perm = reinterpret_cast<int*>(p);
+        p += kSparseMax * 4;
+        S.ipos = reinterpret_cast<int*>(p);
+        p += kSparseMax * 4;
+        S.cstart = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.lvl_nodes = reinterpret_cast<int*>(p);
+        p += kSparseMax * 4;
+        S.height = reinterpret_cast<int*>(p);
+        p += kSparseMax * 4;
+        S.lvl_start = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.rowptr = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.rowidx = reinterpret_cast<int*>(p);
+        p += kRowCap * 4;
+        S.meta = reinterpret_cast<int*>(p);
+        p += 8 * 4;
+        S.Dg = reinterpret_cast<double*>(p);
+        p += kSparseMax * 36 * 8;
+        S.Ld = reinterpret_cast<double*>(p);
+        p += kSparseMax * 36 * 8;
+        S.Ldi = reinterpret_cast<double*>(p);
+        p += kSparseMax * 6 * 8;
+        S.y = reinterpret_cast<double*>(p);
+        p += kSparseMax * 6 * 8;
+        S.z = reinterpret_cast<double*>(p);
+        p += kSparseMax * 6 * 8;
+        S.x = reinterpret_cast<double*>(p);
+        p += kSparseMax * 6 * 8;
+        S.L = reinterpret_cast<double*>(p);
+        const long long used = (p - reinterpret_cast<char*>(B.dense + (long long)T.slot * B.dense_stride)) / 8;
+        S.cap = (int)((B.dense_stride - used) / 36);
+        return S;
+    }
+    // rank of node u among the set bits of a column pattern (= its block slot)
+    __device__ __forceinline__ static int bit_rank(const uint32_t* w, int u) {
+        int r = 0;
+        for (int k = 0; k < (u >> 5); ++k) r += __popc(w[k]);
+        return r + __popc(w[u >> 5] & ((1u << (u & 31)) - 1u));
+    }
+    // node of the a-th set bit of a column pattern
+    __device__ __forceinline__ static int bit_select(const uint32_t* w, int a) {
+        for (int k = 0; k < kSparseWords; ++k) {
+            const int c = __popc(w[k]);
+            if (a < c) {
+                uint32_t x = w[k];
+                for (int q = 0; q < a; ++q) x &= x - 1;
+                return (k << 5) + __ffs(x) - 1;
+            }
+            a -= c;
+        }
+        return -1;
+    }
 
-    // Row-block of active body gb in the dense Newton matrix: the diagonal block P
-    // and, per incidence, the off-diagonal block T_b K^-1 T_o^T =
-    // -[[W, W C_o^T], [C_b W, C_b W C_o^T]] (the 4 blocks of linsysAddition, :232-247).
+    // Symbolic factorisation, once per step: node adjacency from the incidence
+    // lists, greedy minimum-degree elimination on bitsets (ties to the smallest
+    // node), column patterns and block offsets.  Returns false (the scene then
+    // uses PCG) if the factor does not fit the scratch.
+    __device__ bool sparse_symbolic() {
+        Sparse S = sparse_ws();
+        const int n = n_active;
+        for (int q = tid; q < n * kSparseWords; q += nt) S.adj[q] = 0;
+        for (int q = tid; q < n; q += nt) S.ipos[q] = -1;
+        T.sync();
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            if (!active(gb)) continue;
+            const int i = B.didx[gb];
+            const int st0 = B.inc_start[gb], cnt = B.inc_cnt[gb];
+            for (int k = 0; k < cnt; ++k) {
+                const int e = B.inc[st0 + k];
+                const int go = b0 + B.cbody[2 * (e >> 1) + (1 - (e & 1))];
+                if (go == gb || !active(go)) continue;
+                const int j = B.didx[go];
+                S.adj[i * kSparseWords + (j >> 5)] |= 1u << (j & 31);
+            }
+        }
+        T.sync();
+        for (int k = 0; k < n; ++k) {
+            // argmin (degree, node) over the remaining nodes
+            double best[8] = {-1e300, 0, 0, 0, 0, 0, 0, 0};
+            for (int i = tid; i < n; i += nt) {
+                if (S.ipos[i] >= 0) continue;
+                int d = 0;
+                for (int w = 0; w < kSparseWords; ++w) d += __popc(S.adj[i * kSparseWords + w]);
+                const double key = -(double)(d * 65536 + i);
+                best[0] = dmax(best[0], key);
+            }
+            T.max(best);
+            const int v = ((int)(-best[0])) & 65535;
+            const uint32_t* av = S.adj + v * kSparseWords;
+            for (int u = tid; u < n; u += nt) {
+                if (!((av[u >> 5] >> (u & 31)) & 1u)) continue;
+                uint32_t* au = S.adj + u * kSparseWords;
+                for (int w = 0; w < kSparseWords; ++w) au[w] |= av[w];
+                au[u >> 5] &= ~(1u << (u & 31));
+                au[v >> 5] &= ~(1u << (v & 31));
+            }
+            if (tid == 0) {
+                S.perm[k] = v;
+                S.ipos[v] = k;
+            }
+            T.sync();
+        }
+        // block offsets in elimination order
+        if (tid == 0) {
+            int acc = 0;
+            for (int k = 0; k < n; ++k) {
+                const int v = S.perm[k];
+                S.cstart[v] = acc;
+                for (int w = 0; w < kSparseWords; ++w) acc += __popc(S.adj[v * kSparseWords + w]);
+            }
+            S.cstart[n] = acc;
+            if (acc <= S.cap && acc <= kRowCap) {
+                // row lists: for node u, the columns d (in elimination order)
+                // whose pattern contains u, i.e. the blocks L(u, d)
+                for (int v = 0; v <= n; ++v) S.rowptr[v] = 0;
+                for (int d = 0; d < n; ++d)
+                    for (int w = 0; w < kSparseWords; ++w) {
+                        uint32_t bits = S.adj[d * kSparseWords + w];
+                        while (bits) {
+                            S.rowptr[(w << 5) + __ffs(bits)]++;
+                            bits &= bits - 1;
+                        }
+                    }
+                for (int v = 0; v < n; ++v) S.rowptr[v + 1] += S.rowptr[v];
+                for (int v = 0; v < n; ++v) S.height[v] = S.rowptr[v];  // fill cursors
+                for (int k = 0; k < n; ++k) {
+                    const int d = S.perm[k];
+                    for (int w = 0; w < kSparseWords; ++w) {
+                        uint32_t bits = S.adj[d * kSparseWords + w];
+                        while (bits) {
+                            const int u = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            S.rowidx[S.height[u]++] = d;
+                        }
+                    }
+                }
+                // elimination-tree heights: a column can be factorised once every
+                // column that updates it is done; equal heights are independent
+                int nlev = 0;
+                for (int k = 0; k < n; ++k) {
+                    const int v = S.perm[k];
+                    int h = 0;
+                    for (int q = S.rowptr[v]; q < S.rowptr[v + 1]; ++q) h = max(h, S.height[S.rowidx[q]] + 1);
+                    S.height[v] = h;
+                    nlev = max(nlev, h + 1);
+                }
+                for (int l = 0; l <= nlev; ++l) S.lvl_start[l] = 0;
+                for (int v = 0; v < n; ++v) S.lvl_start[S.height[v] + 1]++;
+                for (int l = 0; l < nlev; ++l) S.lvl_start[l + 1] += S.lvl_start[l];
+                int pos = 0;  // stable in elimination order
+                for (int l = 0; l < nlev; ++l)
+                    for (int k = 0; k < n; ++k)
+                        if (S.height[S.perm[k]] == l) S.lvl_nodes[pos++] = S.perm[k];
+                S.meta[0] = nlev;
+            }
+        }
+        T.sync();
+        return S.cstart[n] <= S.cap && S.cstart[n] <= kRowCap;
+    }
+
+    // Column block of active body gb: the diagonal block P and, per incidence
+    // with a body eliminated later, the off-diagonal block T_o K^-1 T_b^T
+    // (linsysAddition's four blocks, :232-247).  Each column is owned by its
+    // body's thread, so accumulation is race free and in incidence order.
     __device__ void assemble_dense_rows(int gb, const double* P) const {
-        const int n6 = 6 * n_active;
-        const int ib = B.didx[gb];
-        double* rows = dense_A() + (long long)(6 * ib) * n6;
+        Sparse S = sparse_ws();
+        const int i = B.didx[gb];
+        double* D = S.Dg + 36 * i;
         for (int r = 0; r < 6; ++r)
-            for (int j = 0; j < n6; ++j) rows[r * n6 + j] = 0.0;
-        for (int r = 0; r < 6; ++r)
-            for (int c = 0; c < 6; ++c) rows[r * n6 + 6 * ib + c] = P[pk(r, c)];
+            for (int c = 0; c < 6; ++c) D[r * 6 + c] = P[pk(r, c)];
+        const uint32_t* ai = S.adj + i * kSparseWords;
+        int m = 0;
+        for (int w = 0; w < kSparseWords; ++w) m += __popc(ai[w]);
+        double* col = S.L + 36LL * S.cstart[i];
+        for (int q = 0; q < 36 * m; ++q) col[q] = 0.0;
         const int st0 = B.inc_start[gb], n = B.inc_cnt[gb];
         for (int k = 0; k < n; ++k) {
             const int e2 = B.inc[st0 + k];
             const int gc = e2 >> 1, side = e2 & 1;
             const int go = b0 + B.cbody[2 * gc + (1 - side)];
             if (!active(go) || go == gb) continue;
-            const int io = B.didx[go];
+            const int j = B.didx[go];
+            if (S.ipos[j] < S.ipos[i]) continue;  // that block lives in j's column
+            double* blk = col + 36 * bit_rank(ai, j);
+            // block (rows o, cols b) = -[[W, C_b W]^T-form]: the transpose of
+            // A_bo = -[[W, W C_o^T], [C_b W, C_b W C_o^T]]
             const double* W = B.W + 6 * gc;
             const d3 cb = ld3(B.arm + 6 * gc + 3 * side);
             const d3 co = ld3(B.arm + 6 * gc + 3 * (1 - side));
             const d3 wr[3] = {d3{W[0], W[3], W[4]}, d3{W[3], W[1], W[5]}, d3{W[4], W[5], W[2]}};
             const d3 y0 = cross3(cb, wr[0]), y1 = cross3(cb, wr[1]), y2 = cross3(cb, wr[2]);
             const d3 yr[3] = {d3{y0.x, y1.x, y2.x}, d3{y0.y, y1.y, y2.y}, d3{y0.z, y1.z, y2.z}};
-            for (int i = 0; i < 3; ++i) {
-                const d3 tr = cross3(co, wr[i]);
-                double* row = rows + (long long)i * n6 + 6 * io;
-                row[0] -= wr[i].x; row[1] -= wr[i].y; row[2] -= wr[i].z;
-                row[3] -= tr.x; row[4] -= tr.y; row[5] -= tr.z;
-                const d3 br = cross3(co, yr[i]);
-                row = rows + (long long)(3 + i) * n6 + 6 * io;
-                row[0] -= yr[i].x; row[1] -= yr[i].y; row[2] -= yr[i].z;
-                row[3] -= br.x; row[4] -= br.y; row[5] -= br.z;
+            for (int r = 0; r < 3; ++r) {
+                const d3 tr = cross3(co, wr[r]);  // row r of W C_o^T
+                const d3 br = cross3(co, yr[r]);  // row r of C_b W C_o^T
+                // A_bo(r, 0..2) = -wr[r], A_bo(r, 3..5) = -tr, A_bo(3+r, 0..2) = -yr[r], A_bo(3+r, 3..5) = -br
+                // stored transposed: blk(c, r) = A_bo(r, c)
+                blk[0 * 6 + r] -= wr[r].x; blk[1 * 6 + r] -= wr[r].y; blk[2 * 6 + r] -= wr[r].z;
+                blk[3 * 6 + r] -= tr.x;    blk[4 * 6 + r] -= tr.y;    blk[5 * 6 + r] -= tr.z;
+                blk[0 * 6 + 3 + r] -= yr[r].x; blk[1 * 6 + 3 + r] -= yr[r].y; blk[2 * 6 + 3 + r] -= yr[r].z;
+                blk[3 * 6 + 3 + r] -= br.x;    blk[4 * 6 + 3 + r] -= br.y;    blk[5 * 6 + 3 + r] -= br.z;
             }
         }
     }
 
-    // Jacobi-scaled dense Cholesky solve of the Newton system (stands in for the
-    // SimplicialLDLT of the direct branch, :359-394).  Writes du; returns false on
-    // a non-positive pivot (the caller then sets du = 0, as :390-394).
+    // Lower Cholesky factor of a 6x6 SPD block (row-major) and the reciprocals
+    // of its diagonal; false if not SPD.
+    __device__ __forceinline__ static bool chol6(const double* A, double* L, double* Li) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            double d = A[j * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) d -= L[j * 6 + k] * L[j * 6 + k];
+            if (!(d > 0.0)) return false;
+            const double ljj = sqrt(d);
+            const double inv = 1.0 / ljj;
+            L[j * 6 + j] = ljj;
+            Li[j] = inv;
+#pragma unroll
+            for (int i = j + 1; i < 6; ++i) {
+                double t = A[i * 6 + j];
+#pragma unroll
+                for (int k = 0; k < j; ++k) t -= L[i * 6 + k] * L[j * 6 + k];
+                L[i * 6 + j] = t * inv;
+            }
+#pragma unroll
+            for (int c = j + 1; c < 6; ++c) L[j * 6 + c] = 0.0;
+        }
+        return true;
+    }
+    // y = L^-1 b
+    __device__ __forceinline__ static void lsolve6(const double* L, const double* Li, const double* b, double* y) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            double t = b[i];
+#pragma unroll
+            for (int k = 0; k < i; ++k) t -= L[i * 6 + k] * y[k];
+            y[i] = t * Li[i];
+        }
+    }
+    // x = L^-T y
+    __device__ __forceinline__ static void ltsolve6(const double* L, const double* Li, const double* y, double* x) {
+#pragma unroll
+        for (int i = 5; i >= 0; --i) {
+            double t = y[i];
+#pragma unroll
+            for (int k = i + 1; k < 6; ++k) t -= L[k * 6 + i] * x[k];
+            x[i] = t * Li[i];
+        }
+    }
+    // C -= A B^T for 6x6 row-major blocks
+    __device__ __forceinline__ static void sub_abt6(double* Cm, const double* A, const double* Bm) {
+        for (int r = 0; r < 6; ++r) {
+            double a[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) a[q] = A[6 * r + q];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) t += a[q] * Bm[6 * c + q];
+                Cm[6 * r + c] -= t;
+            }
+        }
+    }
+
+    // Block Cholesky factorisation + solve of the Newton system: left-looking,
+    // one elimination-tree level at a time (columns of a level are independent;
+    // one team sync per level in each of factor / forward / backward), so a pile
+    // of short stacks takes as many sequential steps as its tallest stack.
+    // Stands in for the direct branch's SimplicialLDLT (:385-394).  Writes du;
+    // false on a non-SPD pivot.
     __device__ bool dense_solve() {
-        const int n = 6 * n_active;
-        const int NM = 6 * C.dense_max;
-        double* A = dense_A();
-        double* x = A + (long long)NM * NM;
-        double* y = x + NM;
-        double* D = y + NM;
-        for (int i = tid; i < n; i += nt) {
-            const int gb = B.dbody[b0 + i / 6];
-            const double d = 1 / sqrt(A[(long long)i * n + i]);
-            D[i] = d;
-            x[i] = B.rhs[6 * gb + i % 6] * d;
-        }
-        __syncthreads();
-        for (long long idx = tid; idx < (long long)n * n; idx += nt) {
-            const int i = (int)(idx / n), j = (int)(idx % n);
-            A[idx] *= D[i] * D[j];
-        }
-        __syncthreads();
-        bool ok = true;
-        for (int k = 0; k < n; ++k) {
-            const double akk = A[(long long)k * n + k];
-            if (!(akk > 0)) { ok = false; break; }
-            const double inv = 1.0 / akk;
-            for (int i = k + 1 + tid; i < n; i += nt) {
-                double* Ai = A + (long long)i * n;
-                const double aik = Ai[k] * inv;
-                for (int j = k + 1; j <= i; ++j) Ai[j] -= aik * A[(long long)j * n + k];
-            }
-            __syncthreads();
-        }
-        if (ok) {
-            for (int k = tid; k < n; k += nt) y[k] = sqrt(A[(long long)k * n + k]);
-            __syncthreads();
-            for (int i = tid; i < n; i += nt)
-                for (int k = 0; k <= i; ++k) {
-                    double& a = A[(long long)i * n + k];
-                    a = (i == k) ? y[k] : a / y[k];
+        Sparse S = sparse_ws();
+        const int n = n_active;
+        const int nlev = S.meta[0];
+        int bad = 0;
+        for (int l = 0; l < nlev; ++l) {
+            for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
+                const int v = S.lvl_nodes[q];
+                const uint32_t* av = S.adj + v * kSparseWords;
+                double* colv = S.L + 36LL * S.cstart[v];
+                double D[36];
+                for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
+                for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
+                    const int d = S.rowidx[r];
+                    const uint32_t* ad = S.adj + d * kSparseWords;
+                    const double* cold = S.L + 36LL * S.cstart[d];
+                    const double* Lvd = cold + 36 * bit_rank(ad, v);
+                    sub_abt6(D, Lvd, Lvd);
+                    int a = 0;  // walk pattern(d): u after v -> L(u,v) -= L(u,d) L(v,d)^T
+                    for (int w = 0; w < kSparseWords; ++w) {
+                        uint32_t bits = ad[w];
+                        while (bits) {
+                            const int u = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (u != v && S.ipos[u] > S.ipos[v])
+                                sub_abt6(colv + 36 * bit_rank(av, u), cold + 36 * a, Lvd);
+                            ++a;
+                        }
+                    }
                 }
-            __syncthreads();
-            for (int k = 0; k < n; ++k) {  // L y = x
-                const double yk = x[k] / A[(long long)k * n + k];
-                if (tid == 0) y[k] = yk;
-                for (int i = k + 1 + tid; i < n; i += nt) x[i] -= A[(long long)i * n + k] * yk;
-                __syncthreads();
+                double Lvv[36], Li[6];
+                if (!chol6(D, Lvv, Li)) {
+                    bad = 1;
+                    continue;
+                }
+                for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
+                for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
+                int m = 0;
+                for (int w = 0; w < kSparseWords; ++w) m += __popc(av[w]);
+                for (int a = 0; a < m; ++a) {  // L(u,v) = A(u,v) L_vv^-T, row by row
+                    double* blk = colv + 36 * a;
+                    for (int r = 0; r < 6; ++r) {
+                        double row[6];
+                        lsolve6(Lvv, Li, blk + 6 * r, row);
+                        for (int c = 0; c < 6; ++c) blk[6 * r + c] = row[c];
+                    }
+                }
             }
-            for (int k = n - 1; k >= 0; --k) {  // L^T z = y
-                const double* Ak = A + (long long)k * n;
-                const double zk = y[k] / Ak[k];
-                if (tid == 0) x[k] = zk;
-                for (int i = tid; i < k; i += nt) y[i] -= Ak[i] * zk;
-                __syncthreads();
+            double fl[8] = {(double)bad, 0, 0, 0, 0, 0, 0, 0};
+            T.max(fl);  // also the level barrier
+            if (fl[0] > 0) {
+                bad = 1;
+                break;
             }
-            for (int i = tid; i < n; i += nt) {
-                const int gb = B.dbody[b0 + i / 6];
-                B.du[6 * gb + i % 6] = x[i] * D[i];
+            T.sync();
+        }
+        if (!bad) {
+            for (int l = 0; l < nlev; ++l) {  // forward: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
+                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
+                    const int v = S.lvl_nodes[q];
+                    const int gb = B.dbody[b0 + v];
+                    double b6[6], yv[6];
+                    for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r];
+                    for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
+                        const int d = S.rowidx[r];
+                        const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSparseWords, v));
+                        const double* yd = S.y + 6 * d;
+                        for (int i = 0; i < 6; ++i) {
+                            double t = 0.0;
+                            for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
+                            b6[i] -= t;
+                        }
+                    }
+                    lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
+                    for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
+                }
+                T.sync();
+            }
+            for (int l = nlev - 1; l >= 0; --l) {  // backward: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
+                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
+                    const int v = S.lvl_nodes[q];
+                    const uint32_t* av = S.adj + v * kSparseWords;
+                    const double* colv = S.L + 36LL * S.cstart[v];
+                    double r6[6], xv[6];
+                    for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r];
+                    int a = 0;
+                    for (int w = 0; w < kSparseWords; ++w) {
+                        uint32_t bits = av[w];
+                        while (bits) {
+                            const int u = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            const double* blk = colv + 36 * a;
+                            const double* xu = S.x + 6 * u;
+                            for (int c = 0; c < 6; ++c) {
+                                double t = 0.0;
+                                for (int r = 0; r < 6; ++r) t += blk[6 * r + c] * xu[r];
+                                r6[c] -= t;
+                            }
+                            ++a;
+                        }
+                    }
+                    ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
+                    for (int r = 0; r < 6; ++r) S.x[6 * v + r] = xv[r];
+                    const int gb = B.dbody[b0 + v];
+                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = xv[r];
+                }
+                T.sync();
             }
         }
-        __syncthreads();
-        return ok;
+        (void)n;
+        T.sync();
+        return !bad;
     }
 
     // X = W (v1p - v0p) of direction vec (or of z + beta*vec when zvec != null),
@@ -1030,7 +1331,7 @@ class SceneSolver {
                 e[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
                 e[6] += (dlin[0] / lI[0]) * rlv[0] + (dlin[1] / lI[1]) * rlv[1];
             }
-            __syncthreads();
+            T.sync();
             for (int b = tid; b < nb; b += nt) {
                 const int gb = b0 + b;
                 if (!active(gb)) continue;
@@ -1041,7 +1342,7 @@ class SceneSolver {
                 e[0] += r2;
                 for (int r = 0; r < 6; ++r) e[4] += (step * B.du[6 * gb + r]) * ruv[r];
             }
-            red.sum(e);
+            T.sum(e);
             const double inErr = e[0] + e[1] + e[2];
             const double sacIn = e[0] + e[3] + e[2];
             const double gErr = -e[4] + e[5] + e[6];
@@ -1060,7 +1361,7 @@ class SceneSolver {
                         for (int k = 0; k < 3; ++k) B.f[3 * gc + k] = B.fT[3 * gc + k];
                         for (int k = 0; k < 2; ++k) B.lam[2 * gc + k] = B.lT[2 * gc + k];
                     }
-                    __syncthreads();
+                    T.sync();
                     return step;
                 }
                 break;
@@ -1122,7 +1423,7 @@ class SceneSolver {
             mx[1] = dmax(mx[1], dmax(-fn, cone_c(fn, B.f[3 * gc + 1], B.f[3 * gc + 2], cmu(gc))));
             for (int k = 0; k < 3; ++k) B.lforce[3 * gc + k] = B.f[3 * gc + k] * cs * cm;
         }
-        __syncthreads();
+        T.sync();
         for (int b = tid; b < nb; b += nt) {
             const int gb = b0 + b;
             if (!B.local[gb]) continue;
@@ -1132,62 +1433,135 @@ class SceneSolver {
                 B.dang[3 * gb + r] = B.u[6 * gb + 3 + r] * cs - B.ang[3 * gb + r];
             }
         }
-        red.sum(e);
-        red.max(mx);
+        T.sum(e);
+        T.max(mx);
         st.kkt_stationarity = dmax(sqrt(e[0]) / (6.0 * n_local), sqrt(e[1]) / (3.0 * nc));
         st.kkt_complementarity = mx[0];
         st.kkt_cone = mx[1];
         st.char_mass = cm;
         st.char_speed = cs;
         st.n_local_bodies = n_local;
+        st.factor_blocks = dense_mode ? sparse_ws().cstart[n_active] : 0;
+        st.team = (T.size == 32) ? 1 : 0;
         st.status = status;
     }
 };
 
+// Scene queues: a single-block kernel buckets the scenes by contact count
+// (largest first, for load balance) into a CTA queue (large scenes) and a warp
+// queue (small scenes), and resets the two work counters.
+// counts[0] = #CTA scenes, [1] = #warp scenes, [2] = CTA counter, [3] = warp counter.
+__global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant__ BatchPtrs B,
+                                                           const __grid_constant__ EngineCfg C) {
+    __shared__ int hist[2][32];
+    __shared__ int start[2][32];
+    const int ns = B.n_scenes;
+    if (threadIdx.x < 64) (&hist[0][0])[threadIdx.x] = 0;
+    __syncthreads();
+    auto size_of = [&](int s, int& nb, int& nc) {
+        if (B.body_off) {
+            nb = B.body_off[s + 1] - B.body_off[s];
+            nc = B.contact_off[s + 1] - B.contact_off[s];
+        } else {
+            nb = B.single_nb;
+            nc = B.single_nc;
+        }
+    };
+    auto queue_of = [&](int nb, int nc) {
+        return (nc <= C.warp_max_contacts && nb <= C.warp_max_bodies) ? 1 : 0;
+    };
+    auto bucket_of = [&](int nc) { return 31 - min(31, 32 - __clz(nc + 1)); };  // large first
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        int nb, nc;
+        size_of(s, nb, nc);
+        atomicAdd(&hist[queue_of(nb, nc)][bucket_of(nc)], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const int q = threadIdx.x;
+        int acc = 0;
+        for (int b = 0; b < 32; ++b) {
+            start[q][b] = acc;
+            acc += hist[q][b];
+        }
+        B.counts[q] = acc;
+        B.counts[2 + q] = 0;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+        int nb, nc;
+        size_of(s, nb, nc);
+        const int q = queue_of(nb, nc);
+        const int pos = atomicAdd(&start[q][bucket_of(nc)], 1);
+        (q ? B.order_warp : B.order_cta)[pos] = s;
+    }
+}
+
+template <class Team>
+__device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C, Team& T, int s) {
+    SceneSolver<Team> S(B, C, T, s);
+    pdc_stats st;
+    st.status = 0;
+    st.newton_iters = 0;
+    st.pcg_iters = 0;
+    st.ls_trials = 0;
+    st.gd_fallbacks = 0;
+    st.n_local_bodies = 0;
+    st.factor_blocks = 0;
+    st.team = (T.size == 32) ? 1 : 0;
+    st.exit_err = 0;
+    st.kkt_stationarity = 0;
+    st.kkt_complementarity = 0;
+    st.kkt_cone = 0;
+    st.char_mass = 0;
+    st.char_speed = 0;
+    const unsigned long long t0 = S.now();
+    if (S.setup()) {
+        S.newton(st);
+        S.finish(st);
+    } else {
+        st.status = S.status;
+    }
+    if (T.rank == 0) {
+        if (B.stats) B.stats[s] = st;
+        if (B.timers) {
+            atomicAdd(&B.timers[0], S.now() - t0);
+            atomicAdd(&B.timers[1], S.t_build);
+            atomicAdd(&B.timers[2], S.t_solve);
+            atomicAdd(&B.timers[3], S.t_ls);
+        }
+    }
+    T.sync();
+}
+
+// Persistent solve: every CTA first drains the CTA queue (one scene per CTA),
+// then each of its warps drains the warp queue (one scene per warp).
 __global__ void __launch_bounds__(256) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
                                                            const __grid_constant__ EngineCfg C) {
     __shared__ double s_red[2 * 8 * 32];
-    __shared__ int s_scene;
-    BlockReducer<8> red;
-    red.init(s_red);
+    __shared__ int s_int[33];
+    __shared__ int s_q;
+    {
+        CtaTeam T(s_red, s_int);
+        const int n_cta = B.counts[0];
+        for (;;) {
+            if (threadIdx.x == 0) s_q = atomicAdd(&B.counts[2], 1);
+            __syncthreads();
+            const int q = s_q;
+            __syncthreads();
+            if (q >= n_cta) break;
+            run_scene(B, C, T, B.order_cta[q]);
+        }
+    }
+    const int warps = blockDim.x >> 5;
+    WarpTeam W(gridDim.x + blockIdx.x * warps + (threadIdx.x >> 5));
+    const int n_warp = B.counts[1];
     for (;;) {
-        if (threadIdx.x == 0) s_scene = atomicAdd(B.work_counter, 1);
-        __syncthreads();
-        const int q = s_scene;
-        __syncthreads();
-        if (q >= B.n_scenes) break;
-        const int s = B.order ? B.order[q] : q;
-        SceneSolver S(B, C, red, s);
-        pdc_stats st;
-        st.status = 0;
-        st.newton_iters = 0;
-        st.pcg_iters = 0;
-        st.ls_trials = 0;
-        st.gd_fallbacks = 0;
-        st.n_local_bodies = 0;
-        st.exit_err = 0;
-        st.kkt_stationarity = 0;
-        st.kkt_complementarity = 0;
-        st.kkt_cone = 0;
-        st.char_mass = 0;
-        st.char_speed = 0;
-        const unsigned long long t0 = S.now();
-        if (S.setup()) {
-            S.newton(st);
-            S.finish(st);
-        } else {
-            st.status = S.status;
-        }
-        if (threadIdx.x == 0) {
-            if (B.stats) B.stats[s] = st;
-            if (B.timers) {
-                atomicAdd(&B.timers[0], S.now() - t0);
-                atomicAdd(&B.timers[1], S.t_build);
-                atomicAdd(&B.timers[2], S.t_solve);
-                atomicAdd(&B.timers[3], S.t_ls);
-            }
-        }
-        __syncthreads();
+        int q = 0;
+        if (W.rank == 0) q = atomicAdd(&B.counts[3], 1);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= n_warp) break;
+        run_scene(B, C, W, B.order_warp[q]);
     }
 }
 

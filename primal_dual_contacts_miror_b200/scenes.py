@@ -110,6 +110,84 @@ def sliding_sphere(radius=0.5, density=1000.0, vel=(3.0, 0, 0), ang=(0, 0, 0)):
     return sb.build()
 
 
+_FRAME_Z = None
+
+
+def settled_pile(n_boxes, rng, max_height=8, half_range=(0.05, 0.2), vel_noise=0.01, density=1000.0):
+    """Contact set of a settled pile of `n_boxes` boxes (vectorised): columns of
+    equal-size cubes (half-extent ~ U[half_range] per column, density 1000) on a
+    static ground, 4 corner contacts per touching face pair, small residual
+    velocities ~ N(0, vel_noise^2).  This is the per-scene contact problem of a
+    box-drop scene once it has come to rest."""
+    global _FRAME_Z
+    from .geometry import frame_from_normal
+
+    if _FRAME_Z is None:
+        _FRAME_Z = frame_from_normal((0.0, 0.0, 1.0)).reshape(-1)
+    heights = []
+    left = n_boxes
+    while left > 0:
+        h = int(min(left, rng.integers(1, max_height + 1)))
+        heights.append(h)
+        left -= h
+    ncol = len(heights)
+    side = int(math.ceil(math.sqrt(ncol)))
+    half = rng.uniform(*half_range, size=ncol)
+    spacing = 2.5 * half_range[1]
+    col_of = np.repeat(np.arange(ncol), heights)
+    level = np.concatenate([np.arange(h) for h in heights])
+    h_b = half[col_of]
+    cx = (col_of % side) * spacing
+    cy = (col_of // side) * spacing
+    cz = h_b + 2 * h_b * level
+    nb = n_boxes + 1
+    mass = np.empty(nb)
+    inertia = np.zeros((nb, 6))
+    inv_inertia = np.zeros((nb, 6))
+    gm, gi0 = box_mass_properties(GROUND_HALF, density)
+    mass[0] = gm
+    inertia[0, :3] = gi0
+    inv_inertia[0, :3] = 1.0 / gi0
+    m = density * (2 * h_b) ** 3
+    i0 = m / 12 * 2 * (2 * h_b) ** 2
+    mass[1:] = m
+    inertia[1:, 0] = inertia[1:, 1] = inertia[1:, 2] = i0
+    inv_inertia[1:, 0] = inv_inertia[1:, 1] = inv_inertia[1:, 2] = 1.0 / i0
+    pos = np.zeros((nb, 3))
+    pos[0] = (0, 0, -GROUND_HALF[2])
+    pos[1:, 0], pos[1:, 1], pos[1:, 2] = cx, cy, cz
+    vel = np.zeros((nb, 3))
+    ang = np.zeros((nb, 3))
+    vel[1:] = rng.normal(0, vel_noise, (n_boxes, 3))
+    ang[1:] = rng.normal(0, vel_noise, (n_boxes, 3))
+    is_static = np.zeros(nb, np.uint8)
+    is_static[0] = 1
+    # contacts: each box with the body below it (ground for level 0)
+    body_idx = np.arange(1, nb)
+    below = np.where(level == 0, 0, body_idx - 1)
+    sx = np.array([-1, -1, 1, 1], float)
+    sy = np.array([-1, 1, -1, 1], float)
+    nc = 4 * n_boxes
+    b0 = np.repeat(below, 4)
+    b1 = np.repeat(body_idx, 4)
+    hh = np.repeat(h_b, 4)
+    cpos = np.stack([np.repeat(cx, 4) + np.tile(sx, n_boxes) * hh,
+                     np.repeat(cy, 4) + np.tile(sy, n_boxes) * hh,
+                     np.repeat(cz - h_b, 4)], 1)
+    arm = np.concatenate([cpos - pos[b0], cpos - pos[b1]], 1)
+    frame = np.tile(_FRAME_Z, (nc, 1))
+    return HostScene(vel, ang, mass, inertia, inv_inertia, is_static, np.stack([b0, b1], 1).astype(np.int32),
+                     frame, arm, np.zeros(nc))
+
+
+def pile_batch(n_scenes, seed, n_min=4, n_max=256, **kw):
+    """Scenes with body counts log-uniform in [n_min, n_max] (the batched
+    4096-scene workload's size distribution)."""
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_scenes))).astype(int)
+    return [settled_pile(int(n), rng, **kw) for n in ns]
+
+
 def box_columns(n_columns, max_height, seed, size_range=(0.5, 1.5), vel_noise=0.05, spacing=2.0,
                 tilt=0.02):
     """Several stacks of boxes on one ground with random heights, sizes and small
