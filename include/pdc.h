@@ -207,6 +207,26 @@ int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
                           double* dvel, double* dang_vel, double* local_force,
                           pdc_stats* stats, void* stream);
 
+/* Allocation-free solve of one scene.  This entry point has no counterpart in
+ * the reference.  It exists for callers that cannot allocate device memory while
+ * stepping: a physics step recorded into a CUDA graph (cudaMalloc cannot be
+ * captured), an engine that owns all device memory through its own pool or
+ * budget, or a real-time loop that cannot afford an allocation's latency or
+ * failure.  It needs no handle and calls no cudaMalloc/cudaFree: its scratch is
+ * a fixed 2 MiB array inside the library (every GPU that loads the library holds
+ * it until exit).  Every pointer in bodies/contacts/out is a DEVICE pointer the
+ * caller owns (is_static and depth required); the work is enqueued on `stream`
+ * (NULL = legacy default stream) on the calling thread's current device.
+ * Limits: at most 256 bodies and 2048 contacts, else PDC_EINVAL.  All calls share
+ * the scratch and it keeps the last call's contents (the kernels reset what must
+ * start at zero), so calls that overlap on the GPU race: serialise them.  The
+ * first call on each device performs a one-time set-up (it looks up the scratch's
+ * device address); make it before any stream capture.  out->stats is zeroed, not
+ * filled.  Errors are reported through pdc_last_error(NULL). */
+int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
+                      const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
+                      pdc_result* out, void* stream);
+
 /* Wait for the handle's outstanding work (bounded: PDC_ETIMEOUT after timeout_ms). */
 int pdc_sync(pdc_solver* s, int32_t timeout_ms);
 

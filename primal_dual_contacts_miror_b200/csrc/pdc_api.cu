@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -525,3 +526,124 @@ extern "C" const char* pdc_last_error(const pdc_solver* s) {
 }
 
 extern "C" const char* pdc_version(void) { return "pdc-b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// Allocation-free single-scene solve.
+//
+// Some callers cannot allocate device memory at solve time: a physics step
+// recorded into a CUDA graph (cudaMalloc is not capturable), a host engine that
+// owns all device memory through its own pool or budget, or a real-time loop
+// where an allocation's latency or failure is not acceptable.  For them this
+// entry point runs the same planner and solve kernels on a fixed scratch area
+// that lives in the library image itself (a file-scope __device__ array), so it
+// never calls cudaMalloc/cudaFree.  The caller still provides every input and
+// output buffer (device pointers).
+//
+// Limits: at most kNoAllocMaxBodies bodies and kNoAllocMaxContacts contacts
+// per call; larger scenes are rejected with PDC_EINVAL.  Every GPU that loads
+// the library holds the 2 MiB array until the process exits.  All calls share
+// it and it keeps the last call's contents: the planner kernel resets the work
+// counters and each solve initialises every scratch value it reads, so nothing
+// needs clearing between calls -- but calls that overlap on the GPU (different
+// streams, threads or processes sharing the context) race on it.  The first
+// call on a device looks up the array's device address (cudaGetSymbolAddress,
+// once per device, with that device current); make that first call before any
+// stream capture.
+namespace {
+constexpr int kNoAllocMaxBodies = 256;
+constexpr int kNoAllocMaxContacts = 2048;
+constexpr long long kNoAllocSparseDoubles = kSparseHeaderDoubles + 36LL * 1024;  // one team slot
+constexpr long long kNoAllocDoubles = 262144;                                     // 2 MiB
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
+                                 const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts, pdc_result* out,
+                                 void* stream) {
+    int rc = validate_config(nullptr, cfg);
+    if (rc) return rc;
+    if (!gravity || !bodies || !contacts || !out || !out->dvel || !out->dang_vel || !out->local_force)
+        return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: null argument");
+    if (!bodies->is_static || !contacts->depth)
+        return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: is_static and depth are required");
+    if (bodies->n < 0 || contacts->n < 0 || !(dt > 0))
+        return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: bad size or time step");
+    if (bodies->n > kNoAllocMaxBodies || contacts->n > kNoAllocMaxContacts)
+        return fail(nullptr, PDC_EINVAL,
+                    "pdc_solve_noalloc: scene exceeds the fixed scratch (max 256 bodies, 2048 contacts)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, PDC_ENODEV, std::string("pdc_solve_noalloc: no device: ") + cudaGetErrorString(e));
+    }
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: device ordinal");
+    double* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {  // once per device, with that device current
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return fail(nullptr, PDC_ECUDA,
+                            std::string("pdc_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            }
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    // carve the workspace out of the fixed array: solver arrays, then one
+    // sparse-factor slot (the scene runs on a single thread block, team slot 0)
+    pdc::BatchPtrs P;
+    std::memset(&P, 0, sizeof(P));
+    Arena A;
+    A.base = base;
+    A.cap = kNoAllocDoubles * sizeof(double);
+    const size_t used = carve(A, 1, std::max(bodies->n, 1), std::max(contacts->n, 1), &P, false, 1, 0);
+    const size_t sparse_off = (used + 255) & ~size_t(255);
+    if (sparse_off + kNoAllocSparseDoubles * sizeof(double) > A.cap)
+        return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: scene exceeds the fixed scratch");
+    P.dense = reinterpret_cast<double*>(reinterpret_cast<char*>(base) + sparse_off);
+    P.dense_stride = kNoAllocSparseDoubles;
+    P.n_scenes = 1;
+    P.body_off = nullptr;
+    P.single_nb = bodies->n;
+    P.single_nc = contacts->n;
+    P.single_dt = dt;
+    for (int k = 0; k < 3; ++k) P.single_g[k] = gravity[k];
+    P.vel = bodies->vel;
+    P.ang = bodies->ang_vel;
+    P.mass = bodies->mass;
+    P.inertia = bodies->inertia;
+    P.inv_inertia = bodies->inv_inertia;
+    P.is_static = bodies->is_static;
+    P.cbody = contacts->body;
+    P.frame = contacts->frame;
+    P.arm = contacts->arm;
+    P.depth = contacts->depth;
+    P.cmu = contacts->mu;
+    P.dvel = out->dvel;
+    P.dang = out->dang_vel;
+    P.lforce = out->local_force;
+    P.stats = nullptr;
+    P.timers = nullptr;
+    std::memset(&out->stats, 0, sizeof(out->stats));
+    pdc::EngineCfg C = engine_cfg(*cfg);
+    C.warp_max_contacts = 0;  // one thread block: only team slot 0 of the sparse scratch is used
+    C.warp_max_bodies = 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        pdc::solve_scenes_kernel<<<1, kThreads, 0, st>>>(P, C);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess)
+        return fail(nullptr, PDC_ECUDA, std::string("pdc_solve_noalloc: launch: ") + cudaGetErrorString(e));
+    return PDC_OK;
+}
