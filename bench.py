@@ -116,6 +116,27 @@ def build_workload(n_scenes, seed):
     return abi.HostBatch(sc, 0.01, (0.0, 0.0, -9.81))
 
 
+def rank_seed(rank):
+    """Each rank solves its own scenes (weak scaling): disjoint seeds per rank."""
+    return SEED + 7919 * rank
+
+
+def max_over_ranks(value, world, device):
+    """Max of a per-rank time over all ranks (collective; every rank calls it)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(n_scenes_per_rank, world, seconds_max, steps):
+    """Whole-job scene-steps/s: all ranks' scenes over the slowest rank's time."""
+    return n_scenes_per_rank * world * steps / seconds_max
+
+
 def cpu_reference(batch, cfg, sample, nthreads):
     """Time the CPU restatement (scene-parallel OpenMP) on the first `sample` scenes."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -191,7 +212,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg.device = local
     solver = lib.Solver(cfg)
-    batch = build_workload(args.scenes, SEED + 7919 * rank)
+    batch = build_workload(args.scenes, rank_seed(rank))
     dev = lib.DeviceBatch(batch, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -220,12 +241,9 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, f"cuda:{local}")
     per_step_s = ms_max / 1e3 / args.steps
-    value = args.scenes * world / per_step_s
+    value = aggregate(args.scenes, world, ms_max / 1e3, args.steps)
     newton = sum(s["newton_iters"] for s in stats)
     ci = float(np.sum(n_contacts * np.array([s["newton_iters"] for s in stats])))
 
@@ -241,10 +259,7 @@ def main():
     for _ in range(e2e_steps):
         solver.batch_solve(batch)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    et = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_value = args.scenes * world / float(et.item())
+    e2e_value = aggregate(args.scenes, world, max_over_ranks(e2e_s, world, f"cuda:{local}"), 1)
 
     peak, peak_kind = load_peaks()
     ab = algorithmic_bytes(stats, n_contacts)
