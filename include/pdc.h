@@ -227,6 +227,55 @@ int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
                       const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
                       pdc_result* out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Device-resident time stepping (DynamicSystem::step, src/Dynamics/DynamicSystem.cpp:130-218,
+ * fixed time step): contact detection (replacing FCL, DynamicSystem.cpp:219-227, with
+ * analytic box/sphere/plane tests and the reference's post-processing, :247-383), the
+ * solve, and integration (updateObjects, :137-161) for many independent scenes, every
+ * step captured once in a CUDA graph and replayed.
+ * Shapes: boxes and spheres are the reference's Cube / Sphere objects
+ * (src/CollisionObject/Cube.cpp, Sphere.cpp); planes are static half-spaces
+ * {x : (x - pos) . n <= 0} with n = the orientation's +z axis (the reference models
+ * ground and walls as static boxes, which also work here). */
+enum pdc_shape_type { PDC_SHAPE_BOX = 0, PDC_SHAPE_SPHERE = 1, PDC_SHAPE_PLANE = 2 };
+
+typedef struct pdc_shapes_soa {
+    int32_t n;
+    const int32_t* type;      /* enum pdc_shape_type */
+    const double* size;       /* [n][3] box half extents; sphere radius in [0] */
+    const double* pos;        /* [n][3] centre of mass (plane: a point on it) */
+    const double* quat;       /* [n][4] orientation x, y, z, w */
+    const double* vel;        /* [n][3] */
+    const double* ang_vel;    /* [n][3] */
+    const double* mass;       /* [n] */
+    const double* inertia0;   /* [n][3] principal moments in the body frame */
+    const uint8_t* is_static; /* [n] */
+} pdc_shapes_soa;
+
+typedef struct pdc_world pdc_world;
+
+/* n_scenes scenes; scene k owns bodies [body_offsets[k], body_offsets[k+1]).  Each
+ * scene gets contacts_per_body * n_bodies + 16 contact slots (points beyond are
+ * dropped and counted, see pdc_world_stats). */
+int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const int32_t* body_offsets,
+                     const double* dt, const double* gravity, const pdc_shapes_soa* shapes,
+                     int32_t contacts_per_body, pdc_world** out);
+void pdc_world_destroy(pdc_world* w);
+/* Enqueue n_steps steps on `stream` (NULL: the world's own stream). */
+int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream);
+/* Contact detection only, at the current poses (synchronous). */
+int pdc_world_collide(pdc_world* w);
+/* Bounded wait for the world's work (PDC_ETIMEOUT after timeout_ms). */
+int pdc_world_sync(pdc_world* w, int32_t timeout_ms);
+/* Copy body state out (any pointer may be NULL). */
+int pdc_world_state(pdc_world* w, double* pos, double* quat, double* vel, double* ang_vel);
+/* Copy the last contact sets out, scene by scene, compacted: counts[n_scenes], then
+ * per contact body[2] (scene-local), frame[9], arm[6], depth, pos[3], local_force[3]. */
+int pdc_world_contacts(pdc_world* w, int32_t* counts, int32_t* body, double* frame, double* arm,
+                       double* depth, double* pos, double* local_force);
+/* Per-scene solver statistics of the last step and dropped contact points. */
+int pdc_world_stats(pdc_world* w, pdc_stats* stats, int32_t* overflow);
+
 /* Wait for the handle's outstanding work (bounded: PDC_ETIMEOUT after timeout_ms). */
 int pdc_sync(pdc_solver* s, int32_t timeout_ms);
 

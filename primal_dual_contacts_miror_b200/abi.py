@@ -119,6 +119,65 @@ class Batch(C.Structure):
     ]
 
 
+PDC_SHAPE_BOX, PDC_SHAPE_SPHERE, PDC_SHAPE_PLANE = 0, 1, 2
+
+
+class Shapes(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("type", _ip),
+        ("size", _dp),
+        ("pos", _dp),
+        ("quat", _dp),
+        ("vel", _dp),
+        ("ang_vel", _dp),
+        ("mass", _dp),
+        ("inertia0", _dp),
+        ("is_static", _u8p),
+    ]
+
+
+class ShapeBatch:
+    """Bodies of many scenes (shape, pose, velocity, mass) for the device world,
+    packed by scene (scene k owns bodies body_offsets[k]:body_offsets[k+1])."""
+
+    def __init__(self, scenes, dt, gravity):
+        c = np.ascontiguousarray
+        cat = lambda key, dtype: c(np.concatenate([np.asarray(s[key], dtype=dtype) for s in scenes]), dtype=dtype)
+        self.type = cat("type", np.int32)
+        self.size = cat("size", np.float64).reshape(-1, 3)
+        self.pos = cat("pos", np.float64).reshape(-1, 3)
+        self.quat = cat("quat", np.float64).reshape(-1, 4)
+        self.vel = cat("vel", np.float64).reshape(-1, 3)
+        self.ang_vel = cat("ang_vel", np.float64).reshape(-1, 3)
+        self.mass = cat("mass", np.float64)
+        self.inertia0 = cat("inertia0", np.float64).reshape(-1, 3)
+        self.is_static = cat("is_static", np.uint8)
+        ns = len(scenes)
+        self.body_offsets = np.zeros(ns + 1, np.int32)
+        self.body_offsets[1:] = np.cumsum([len(s["type"]) for s in scenes])
+        self.dt = c(np.broadcast_to(np.asarray(dt, np.float64), (ns,)))
+        self.gravity = c(np.broadcast_to(np.asarray(gravity, np.float64).reshape(-1, 3), (ns, 3)))
+        self.scenes = scenes
+
+    @property
+    def n(self):
+        return int(self.type.shape[0])
+
+    @property
+    def n_scenes(self):
+        return len(self.scenes)
+
+    @staticmethod
+    def ptr(a, ct=C.c_double):
+        return a.ctypes.data_as(C.POINTER(ct))
+
+    def struct(self):
+        p = self.ptr
+        return Shapes(self.n, p(self.type, C.c_int32), p(self.size), p(self.pos), p(self.quat), p(self.vel),
+                      p(self.ang_vel), p(self.mass), p(self.inertia0), p(self.is_static, C.c_uint8))
+
+
 def default_config(**overrides):
     """The reference's YAML defaults (PrimalDualForceSolver.cpp:650-652,
     NonSmoothContactForce.cpp:320-334) plus this library's solver knobs."""

@@ -647,3 +647,5 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
         return fail(nullptr, PDC_ECUDA, std::string("pdc_solve_noalloc: launch: ") + cudaGetErrorString(e));
     return PDC_OK;
 }
+
+#include "pdc_world.cuh"

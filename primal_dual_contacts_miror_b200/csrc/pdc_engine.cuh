@@ -49,6 +49,7 @@ struct BatchPtrs {
     double single_dt, single_g[3];
     const int* __restrict__ body_off;
     const int* __restrict__ contact_off;
+    const int* __restrict__ contact_cnt;  // optional: contacts used in each slice (else the slice size)
     const double* __restrict__ dt;
     const double* __restrict__ grav;
     // bodies (inputs)
@@ -171,7 +172,7 @@ class SceneSolver {
             b0 = B.body_off[s];
             nb = B.body_off[s + 1] - b0;
             c0 = B.contact_off[s];
-            nc = B.contact_off[s + 1] - c0;
+            nc = B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - c0;
             dt = B.dt[s];
             g[0] = B.grav[3 * s];
             g[1] = B.grav[3 * s + 1];
@@ -1461,7 +1462,7 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
     auto size_of = [&](int s, int& nb, int& nc) {
         if (B.body_off) {
             nb = B.body_off[s + 1] - B.body_off[s];
-            nc = B.contact_off[s + 1] - B.contact_off[s];
+            nc = B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - B.contact_off[s];
         } else {
             nb = B.single_nb;
             nc = B.single_nc;

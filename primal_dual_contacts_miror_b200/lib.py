@@ -138,6 +138,101 @@ class Solver:
         self._check(self.lib.pdc_reset(self.h))
 
 
+class World:
+    """Device-resident stepping of many scenes (pdc_world_*): contact detection,
+    solve and integration on the GPU, one CUDA-graph replay per step."""
+
+    def __init__(self, shapes, cfg=None, contacts_per_body=16, **overrides):
+        self.lib = load()
+        _bind_world(self.lib)
+        self.cfg = cfg if cfg is not None else abi.default_config(**overrides)
+        self.shapes = shapes
+        h = C.c_void_p()
+        rc = self.lib.pdc_world_create(C.byref(self.cfg), shapes.n_scenes, shapes.ptr(shapes.body_offsets, C.c_int32),
+                                       shapes.ptr(shapes.dt), shapes.ptr(shapes.gravity), C.byref(shapes.struct()),
+                                       contacts_per_body, C.byref(h))
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+
+    def step(self, n=1, stream=None):
+        self._check(self.lib.pdc_world_step(self.h, n, C.c_void_p(stream or 0)))
+
+    def sync(self, timeout_ms=600000):
+        self._check(self.lib.pdc_world_sync(self.h, timeout_ms))
+
+    def collide(self):
+        self._check(self.lib.pdc_world_collide(self.h))
+
+    def state(self):
+        nb = self.shapes.n
+        pos, quat, vel, ang = np.zeros((nb, 3)), np.zeros((nb, 4)), np.zeros((nb, 3)), np.zeros((nb, 3))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.pdc_world_state(self.h, dp(pos), dp(quat), dp(vel), dp(ang)))
+        return pos, quat, vel, ang
+
+    def contacts(self):
+        ns = self.shapes.n_scenes
+        counts = np.zeros(ns, np.int32)
+        cap = int(self.shapes.n * 64 + 16 * ns)
+        body = np.zeros((cap, 2), np.int32)
+        frame, arm, depth = np.zeros((cap, 9)), np.zeros((cap, 6)), np.zeros(cap)
+        pos, lf = np.zeros((cap, 3)), np.zeros((cap, 3))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.pdc_world_contacts(self.h, counts.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                body.ctypes.data_as(C.POINTER(C.c_int32)), dp(frame), dp(arm),
+                                                dp(depth), dp(pos), dp(lf)))
+        n = int(counts.sum())
+        return counts, {"body": body[:n], "frame": frame[:n], "arm": arm[:n], "depth": depth[:n], "pos": pos[:n],
+                        "local_force": lf[:n]}
+
+    def stats(self):
+        ns = self.shapes.n_scenes
+        st = (abi.Stats * ns)()
+        ov = np.zeros(ns, np.int32)
+        self._check(self.lib.pdc_world_stats(self.h, st, ov.ctypes.data_as(C.POINTER(C.c_int32))))
+        return [s.as_dict() for s in st], ov
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pdc_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _bind_world(lib):
+    if getattr(lib, "_world_bound", False):
+        return
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    lib.pdc_world_create.argtypes = [C.POINTER(abi.Config), C.c_int32, ip, dp, dp, C.POINTER(abi.Shapes), C.c_int32,
+                                     C.POINTER(vp)]
+    lib.pdc_world_create.restype = C.c_int
+    lib.pdc_world_destroy.argtypes = [vp]
+    lib.pdc_world_destroy.restype = None
+    lib.pdc_world_step.argtypes = [vp, C.c_int32, vp]
+    lib.pdc_world_step.restype = C.c_int
+    lib.pdc_world_collide.argtypes = [vp]
+    lib.pdc_world_collide.restype = C.c_int
+    lib.pdc_world_sync.argtypes = [vp, C.c_int32]
+    lib.pdc_world_sync.restype = C.c_int
+    lib.pdc_world_state.argtypes = [vp, dp, dp, dp, dp]
+    lib.pdc_world_state.restype = C.c_int
+    lib.pdc_world_contacts.argtypes = [vp, ip, ip, dp, dp, dp, dp, dp]
+    lib.pdc_world_contacts.restype = C.c_int
+    lib.pdc_world_stats.argtypes = [vp, C.POINTER(abi.Stats), ip]
+    lib.pdc_world_stats.restype = C.c_int
+    lib._world_bound = True
+
+
 class DeviceBatch:
     """A HostBatch copied to device memory (torch tensors keep the storage),
     with the ABI structs pointing at it.  Used by pdc_batch_solve_async."""

@@ -188,6 +188,92 @@ def pile_batch(n_scenes, seed, n_min=4, n_max=256, **kw):
     return [settled_pile(int(n), rng, **kw) for n in ns]
 
 
+# ----------------------------------------------------------------- world scenes
+# Shape-level scenes for the device world (pdc_world_*): dicts of per-body
+# arrays (type, size, pos, quat, vel, ang_vel, mass, inertia0, is_static).
+
+_PLANE_QUATS = {  # orientation whose +z axis is the plane normal
+    "+z": (0.0, 0.0, 0.0, 1.0),
+    "+x": (0.0, math.sqrt(0.5), 0.0, math.sqrt(0.5)),
+    "-x": (0.0, -math.sqrt(0.5), 0.0, math.sqrt(0.5)),
+    "+y": (-math.sqrt(0.5), 0.0, 0.0, math.sqrt(0.5)),
+    "-y": (math.sqrt(0.5), 0.0, 0.0, math.sqrt(0.5)),
+}
+
+
+class ShapeSceneBuilder:
+    def __init__(self):
+        self.rows = []
+
+    def add(self, type_, size, pos, quat=(0, 0, 0, 1), vel=(0, 0, 0), ang=(0, 0, 0), mass=1.0, i0=(1, 1, 1),
+            static=False):
+        self.rows.append((type_, tuple(size), tuple(pos), tuple(quat), tuple(vel), tuple(ang), float(mass),
+                          tuple(i0), 1 if static else 0))
+        return len(self.rows) - 1
+
+    def add_box(self, half, pos, density=1000.0, quat=(0, 0, 0, 1), vel=(0, 0, 0), ang=(0, 0, 0), static=False):
+        m, i0 = box_mass_properties(half, density)
+        return self.add(0, half, pos, quat, vel, ang, m, i0, static)
+
+    def add_sphere(self, radius, pos, density=1000.0, vel=(0, 0, 0), ang=(0, 0, 0), static=False):
+        m, i0 = sphere_mass_properties(radius, density)
+        return self.add(1, (radius, 0, 0), pos, (0, 0, 0, 1), vel, ang, m, i0, static)
+
+    def add_plane(self, point, normal="+z"):
+        return self.add(2, (0, 0, 0), point, _PLANE_QUATS[normal], mass=1.0, i0=(1, 1, 1), static=True)
+
+    def build(self):
+        cols = list(zip(*self.rows))
+        keys = ["type", "size", "pos", "quat", "vel", "ang_vel", "mass", "inertia0", "is_static"]
+        return {k: np.array(v) for k, v in zip(keys, cols)}
+
+
+def stack_world(n_boxes=10, size=1.0, density=1000.0, gap=0.001, ground="box"):
+    """The single-scene workload: n cubes of side `size`, density 1000, stacked on
+    z with `gap` between faces above a static ground whose top is z = 0 (a
+    20 x 20 x 1 m static box, as the reference models ground, or a plane)."""
+    sb = ShapeSceneBuilder()
+    if ground == "box":
+        sb.add_box((10.0, 10.0, 0.5), (0.0, 0.0, -0.5), static=True)
+    else:
+        sb.add_plane((0.0, 0.0, 0.0), "+z")
+    h = size / 2
+    for k in range(n_boxes):
+        sb.add_box((h, h, h), (0.0, 0.0, k * (size + gap) + gap + h), density)
+    return sb.build()
+
+
+def random_quat(rng):
+    q = rng.normal(size=4)
+    return q / np.linalg.norm(q)
+
+
+def box_drop_world(n, rng, half_range=(0.05, 0.2), height=40.0, density=1000.0):
+    """A random box drop: n boxes with half extents i.i.d. U[half_range], density
+    1000, centres i.i.d. uniform in a column of footprint 10 sqrt(n/2000) m
+    square and `height` m tall, uniform random orientations, at rest; static
+    ground and four walls (planes)."""
+    L = 10.0 * math.sqrt(n / 2000.0)
+    sb = ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    sb.add_plane((0.0, 0.0, 0.0), "+x")
+    sb.add_plane((L, 0.0, 0.0), "-x")
+    sb.add_plane((0.0, 0.0, 0.0), "+y")
+    sb.add_plane((0.0, L, 0.0), "-y")
+    for _ in range(n):
+        half = rng.uniform(*half_range, size=3)
+        r = float(np.linalg.norm(half))
+        pos = (rng.uniform(r, max(r, L - r)), rng.uniform(r, max(r, L - r)), rng.uniform(r, height))
+        sb.add_box(tuple(half), pos, density, quat=tuple(random_quat(rng)))
+    return sb.build()
+
+
+def box_drop_batch(n_scenes, seed, n_min=4, n_max=256, **kw):
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_scenes))).astype(int)
+    return [box_drop_world(int(n), rng, **kw) for n in ns]
+
+
 def box_columns(n_columns, max_height, seed, size_range=(0.5, 1.5), vel_noise=0.05, spacing=2.0,
                 tilt=0.02):
     """Several stacks of boxes on one ground with random heights, sizes and small

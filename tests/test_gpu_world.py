@@ -1,0 +1,100 @@
+"""Device world (pdc_world_*) against the host restatement: contact sets equal to
+the numpy contact generation on the same poses, trajectories equal to the host
+pipeline (numpy contacts -> CPU oracle solve -> numpy integration), and the
+10-box stack of the single-scene workload settling."""
+import math
+
+import numpy as np
+import pytest
+
+import world_ref
+from primal_dual_contacts_miror_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def jumbled_scene(rng, n_box=6, n_sph=4, L=1.2):
+    """Boxes and spheres placed at random in a small cube over a ground plane:
+    many overlapping pairs of every kind."""
+    sb = scenes.ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    sb.add_box((2.0, 2.0, 0.25), (0.0, 0.0, -0.2), static=True)
+    for _ in range(n_box):
+        sb.add_box(tuple(rng.uniform(0.1, 0.35, 3)), tuple(rng.uniform([-L / 2, -L / 2, 0.0], [L / 2, L / 2, L])),
+                   quat=tuple(scenes.random_quat(rng)))
+    for _ in range(n_sph):
+        sb.add_sphere(float(rng.uniform(0.1, 0.3)), tuple(rng.uniform([-L / 2, -L / 2, 0.0], [L / 2, L / 2, L])))
+    return sb.build()
+
+
+def test_collide_matches_host_contact_generation():
+    from primal_dual_contacts_miror_b200 import lib
+
+    rng = np.random.default_rng(7)
+    sc = [jumbled_scene(rng) for _ in range(24)]
+    sb = abi.ShapeBatch(sc, 0.01, (0, 0, -9.81))
+    w = lib.World(sb, contacts_per_body=24)
+    w.collide()
+    counts, got = w.contacts()
+    o = 0
+    total = 0
+    for k, s in enumerate(sc):
+        ref = world_ref.npr.collide(s["type"], s["size"], s["pos"], s["quat"], s["is_static"])
+        assert counts[k] == len(ref), (k, counts[k], len(ref))
+        for q, c in enumerate(ref):
+            i = o + q
+            assert tuple(got["body"][i]) == c["body"]
+            np.testing.assert_allclose(got["pos"][i], c["pos"], atol=1e-12)
+            np.testing.assert_allclose(got["frame"][i], c["frame"].reshape(-1), atol=1e-12)
+            np.testing.assert_allclose(got["arm"][i], c["arm"], atol=1e-12)
+            assert got["depth"][i] == pytest.approx(c["depth"], abs=1e-12)
+        o += counts[k]
+        total += len(ref)
+    assert total > 100  # every pair kind exercised
+    w.close()
+
+
+@pytest.mark.parametrize("name", ["stack3", "drop"])
+def test_world_trajectory_matches_host_pipeline(name):
+    from primal_dual_contacts_miror_b200 import lib
+
+    rng = np.random.default_rng(3)
+    if name == "stack3":
+        sc = scenes.stack_world(3, gap=0.001)
+        steps = 30
+    else:
+        sc = jumbled_scene(rng, n_box=3, n_sph=2)
+        steps = 20
+    cfg = abi.default_config(tol=1e-8)
+    w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), cfg=cfg)
+    state = world_ref.initial_state(sc)
+    for _ in range(steps):
+        world_ref.step(sc, state, 0.01, (0, 0, -9.81), cfg)
+    w.step(steps)
+    w.sync()
+    pos, quat, vel, ang = w.state()
+    np.testing.assert_allclose(pos, state[0], atol=1e-7)
+    np.testing.assert_allclose(vel, state[2], atol=1e-6)
+    w.close()
+
+
+def test_c1_ten_box_stack_settles():
+    """10 cubes (1 m, density 1000) with 1 mm gaps on a static ground, mu 0.5,
+    dt 0.01, 200 steps, tol 1e-8: the stack comes to rest in place."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    sc = scenes.stack_world(10, gap=0.001)
+    w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), cfg=abi.default_config(tol=1e-8))
+    w.step(200)
+    w.sync()
+    pos, quat, vel, ang = w.state()
+    counts, cts = w.contacts()
+    st, ov = w.stats()
+    assert ov[0] == 0
+    assert counts[0] == 40  # 4 corner points per face pair
+    assert np.abs(vel[1:]).max() < 1e-3 and np.abs(ang[1:]).max() < 1e-3
+    z = pos[1:, 2]
+    assert np.all(np.diff(z) > 0.99) and np.all(np.diff(z) < 1.01)
+    assert np.abs(pos[1:, :2]).max() < 1e-6
+    assert st[0]["status"] == 0
+    w.close()
