@@ -176,6 +176,40 @@ def run_reference(args, cfg):
     print(json.dumps(line))
 
 
+def run_world(args, cfg, lib, torch, stream, local, rank, world):
+    """The full device pipeline on the batched box-drop workload: 4,096 scenes of
+    n ~ log-uniform[4, 256] boxes dropped in a column of footprint 10 sqrt(n/2000)
+    m (ground + 4 walls), mu 0.5, dt 0.01.  After `world_settle` untimed steps
+    (the piles have formed), `steps` steps of collide + solve + integrate, each a
+    CUDA-graph replay, are timed with events; max over ranks."""
+    shapes = abi.ShapeBatch(scenes.box_drop_batch(args.world_scenes, rank_seed(rank) + 17), 0.01, (0.0, 0.0, -9.81))
+    w = lib.World(shapes, cfg=cfg, contacts_per_body=16)
+    sh = stream.cuda_stream
+    t0 = time.perf_counter()
+    w.step(args.world_settle, sh)
+    torch.cuda.synchronize()
+    settle_s = time.perf_counter() - t0
+    w.step(args.warmup, sh)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    w.step(args.steps, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local}")
+    st, ov = w.stats()
+    counts, _ = w.contacts()
+    w.close()
+    return {"value": aggregate(args.world_scenes, world, ms / 1e3, args.steps), "unit": METRIC,
+            "ms_per_step": ms / args.steps, "bodies_per_gpu": int(shapes.n),
+            "contacts_per_step": int(counts.sum()), "dropped_contact_points": int(ov.sum()),
+            "newton_iters_mean": float(np.mean([s["newton_iters"] for s in st])),
+            "untimed_settle_steps": args.world_settle, "untimed_settle_s": settle_s,
+            "launches_per_step": 5, "workload": f"{args.world_scenes} box drops, 4-256 boxes, dt 0.01, "
+                                                f"timed after {args.world_settle} steps"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,14 +219,20 @@ def main():
     ap.add_argument("--scenes", type=int, default=4096)
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--sparse-max", type=int, default=256)
-    ap.add_argument("--warp-max-contacts", type=int, default=4096)
-    ap.add_argument("--warp-max-bodies", type=int, default=512)
+    ap.add_argument("--warp-max-contacts", type=int, default=0)
+    ap.add_argument("--warp-max-bodies", type=int, default=0)
+    ap.add_argument("--cta-threads", type=int, default=256)
+    ap.add_argument("--world-scenes", type=int, default=4096)
+    ap.add_argument("--world-settle", type=int, default=100)
+    ap.add_argument("--no-world", action="store_true")
+    ap.add_argument("--single-sample", type=int, default=256)
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = abi.default_config(tol=args.tol, sparse_max_bodies=args.sparse_max,
-                             warp_max_contacts=args.warp_max_contacts, warp_max_bodies=args.warp_max_bodies)
+                             warp_max_contacts=args.warp_max_contacts, warp_max_bodies=args.warp_max_bodies,
+                             cta_threads=args.cta_threads)
     if args.impl == "reference":
         run_reference(args, cfg)
         return
@@ -286,6 +326,27 @@ def main():
                      "algorithmic_bytes_per_launch": ab, "kernel": "solve_scenes_kernel"},
         "clocks": clk,
     }
+    # plain FP64 one scene per launch (the one-at-a-time denominator), first scenes
+    ns1 = min(args.single_sample, batch.n_scenes)
+    singles = []
+    for k in range(ns1):
+        sc = batch.scenes[k]
+        singles.append(lib.DeviceBatch(abi.HostBatch([sc], 0.01, (0.0, 0.0, -9.81)), device=f"cuda:{local}"))
+    for d in singles[: min(4, ns1)]:
+        solver.batch_solve_device(d, sh)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for d in singles:
+        solver.batch_solve_device(d, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    line["plain_one_scene_per_launch"] = {"value": ns1 / (e0.elapsed_time(e1) / 1e3), "unit": METRIC,
+                                          "sample": f"first {ns1} scenes, one launch each"}
+    del singles
+
+    if not args.no_world:
+        line["world"] = run_world(args, cfg, lib, torch, stream, local, rank, world)
+
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib

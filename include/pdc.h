@@ -93,7 +93,8 @@ typedef struct pdc_config {
                                   scenes use PCG */
     int32_t warp_max_contacts; /* batched launch: scenes with at most this many contacts */
     int32_t warp_max_bodies;   /* and bodies are solved by one warp, larger ones by a
-                                  whole thread block (4096 / 512; 0 = blocks only) */
+                                  whole thread block (0 / 0 = blocks only, the default) */
+    int32_t cta_threads;       /* threads per block of the solve kernel: 128 or 256 (256) */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
     int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
     double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */
@@ -261,7 +262,8 @@ int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const int32_t* bod
                      const double* dt, const double* gravity, const pdc_shapes_soa* shapes,
                      int32_t contacts_per_body, pdc_world** out);
 void pdc_world_destroy(pdc_world* w);
-/* Enqueue n_steps steps on `stream` (NULL: the world's own stream). */
+/* Enqueue n_steps steps on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream).  The step graph is captured on the first call. */
 int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream);
 /* Contact detection only, at the current poses (synchronous). */
 int pdc_world_collide(pdc_world* w);

@@ -45,6 +45,7 @@ class Config(C.Structure):
         ("sparse_max_bodies", C.c_int32),
         ("warp_max_contacts", C.c_int32),
         ("warp_max_bodies", C.c_int32),
+        ("cta_threads", C.c_int32),
         ("pcg_rtol_direct", C.c_double),
         ("pcg_max_direct", C.c_int32),
         ("pcg_rtol_iter", C.c_double),
@@ -194,8 +195,9 @@ def default_config(**overrides):
     cfg.precision = PDC_PRECISION_FP64
     cfg.direct_threshold = 2000
     cfg.sparse_max_bodies = 256
-    cfg.warp_max_contacts = 4096
-    cfg.warp_max_bodies = 512
+    cfg.warp_max_contacts = 0
+    cfg.warp_max_bodies = 0
+    cfg.cta_threads = 256
     cfg.pcg_rtol_direct = 1e-13
     cfg.pcg_max_direct = 4000
     cfg.pcg_rtol_iter = 1e-8

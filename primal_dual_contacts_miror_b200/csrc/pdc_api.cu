@@ -48,6 +48,7 @@ struct pdc_solver {
     int device = 0;
     int num_sms = 0;
     int blocks_per_sm = 1;
+    int threads = 256;  // threads per block of the solve kernel
     cudaStream_t stream = nullptr;
     Arena arena;
     std::string err;
@@ -208,8 +209,9 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->precision = PDC_PRECISION_FP64;
     c->direct_threshold = 2000;  // :385
     c->sparse_max_bodies = 256;
-    c->warp_max_contacts = 4096;
-    c->warp_max_bodies = 512;
+    c->warp_max_contacts = 0;  // measured: thread blocks win even for small scenes
+    c->warp_max_bodies = 0;
+    c->cta_threads = 256;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;
     c->pcg_rtol_iter = 1e-8;
@@ -251,8 +253,11 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
     e = cudaSetDevice(s->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    s->threads = (cfg->cta_threads == 128) ? 128 : 256;
     if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel, kThreads, 0);
+        e = (s->threads == 128)
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel<128>, 128, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel<256>, 256, 0);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_timers, 4 * sizeof(unsigned long long) + 16);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_counter, 16);
     if (e == cudaSuccess) e = cudaMemset(s->d_timers, 0, 4 * sizeof(unsigned long long));
@@ -297,7 +302,8 @@ static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st) {
     pdc::EngineCfg C = engine_cfg(s->cfg);
     pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
     CK(cudaGetLastError(), "launch plan_scenes_kernel");
-    pdc::solve_scenes_kernel<<<grid, kThreads, 0, st>>>(P, C);
+    if (s->threads == 128) pdc::solve_scenes_kernel<128><<<grid, 128, 0, st>>>(P, C);
+    else pdc::solve_scenes_kernel<256><<<grid, 256, 0, st>>>(P, C);
     CK(cudaGetLastError(), "launch solve_scenes_kernel");
     return PDC_OK;
 }
@@ -640,7 +646,7 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
     pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-        pdc::solve_scenes_kernel<<<1, kThreads, 0, st>>>(P, C);
+        pdc::solve_scenes_kernel<kThreads><<<1, kThreads, 0, st>>>(P, C);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess)

@@ -1537,7 +1537,8 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
 
 // Persistent solve: every CTA first drains the CTA queue (one scene per CTA),
 // then each of its warps drains the warp queue (one scene per warp).
-__global__ void __launch_bounds__(256) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
                                                            const __grid_constant__ EngineCfg C) {
     __shared__ double s_red[2 * 8 * 32];
     __shared__ int s_int[33];

@@ -340,7 +340,8 @@ extern "C" int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream) {
     pdc_solver* s = w->solver;
     if (n_steps < 0) return fail(s, PDC_EINVAL, "negative step count");
     CK(cudaSetDevice(s->device), "cudaSetDevice");
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : w->stream;
+    // NULL is the legacy default stream, as for every CUDA runtime call
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!w->exec) {  // capture one step once, replay it every step after
         CK(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         int rc = world_enqueue_step(w, w->stream);

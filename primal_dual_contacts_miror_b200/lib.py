@@ -240,7 +240,7 @@ class DeviceBatch:
     def __init__(self, batch, device="cuda"):
         import torch
 
-        t = lambda a, dt=None: torch.as_tensor(np.ascontiguousarray(a), device=device)
+        t = lambda a, dt=None: torch.as_tensor(np.array(a, copy=True, order="C"), device=device)
         a = batch.all
         self.keep = {
             "body_off": t(batch.body_offsets), "contact_off": t(batch.contact_offsets), "dt": t(batch.dt),

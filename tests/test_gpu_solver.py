@@ -130,6 +130,21 @@ def test_batch_parity_with_oracle(gpu):
                 (ora[0][b0:b1], ora[1][b0:b1], ora[2][c0:c1], ora[3][k]))
 
 
+def test_warp_teams_match_block_teams(gpu):
+    """Small scenes routed to single-warp teams give the block-team result (the
+    reductions differ in association only)."""
+    sc = [scenes.box_columns(k + 1, 2, seed=300 + k, vel_noise=0.01, tilt=0.0) for k in range(10)]
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    blk = gpu.Solver(abi.default_config(tol=1e-8)).batch_solve(batch)
+    wrp = gpu.Solver(abi.default_config(tol=1e-8, warp_max_contacts=4096, warp_max_bodies=512)).batch_solve(batch)
+    assert all(s["team"] == 1 for s in wrp[3]) and all(s["team"] == 0 for s in blk[3])
+    for k in range(len(sc)):
+        b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
+        c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
+        compare((wrp[0][b0:b1], wrp[1][b0:b1], wrp[2][c0:c1], wrp[3][k]),
+                (blk[0][b0:b1], blk[1][b0:b1], blk[2][c0:c1], blk[3][k]))
+
+
 def test_no_contacts(gpu):
     s = scenes.box_on_ground()
     s2 = abi.HostScene(s.vel, s.ang_vel, s.mass, s.inertia, s.inv_inertia, s.is_static,
