@@ -340,7 +340,29 @@ def main():
         solver.batch_solve_device(d, sh)
     e1.record(stream)
     torch.cuda.synchronize()
-    line["plain_one_scene_per_launch"] = {"value": ns1 / (e0.elapsed_time(e1) / 1e3), "unit": METRIC,
+    single_ms = e0.elapsed_time(e1)
+    # mixed precision (FP32 bulk + FP64 refinement) on the same batch
+    mcfg = abi.default_config(**{n: getattr(cfg, n) for n, _ in abi.Config._fields_})
+    mcfg.precision = abi.PDC_PRECISION_MIXED
+    msolver = lib.Solver(mcfg)
+    for _ in range(args.warmup):
+        msolver.batch_solve_device(dev, sh)
+    torch.cuda.synchronize()
+    mstats = dev.stats_list()
+    e0.record(stream)
+    for _ in range(args.steps):
+        msolver.batch_solve_device(dev, sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    mms = max_over_ranks(e0.elapsed_time(e1), world, f"cuda:{local}")
+    line["mixed"] = {"value": aggregate(args.scenes, world, mms / 1e3, args.steps), "unit": METRIC,
+                     "ms_per_step": mms / args.steps, "dtype": "f32 bulk + f64 refinement",
+                     "newton_iters_mean": float(np.mean([s["newton_iters"] for s in mstats])),
+                     "inner_pcg_iters_mean": float(np.mean([s["pcg_iters"] for s in mstats])),
+                     "scene_status": {str(k): sum(1 for s in mstats if s["status"] == k)
+                                      for k in sorted({s["status"] for s in mstats})}}
+    msolver.close()
+    line["plain_one_scene_per_launch"] = {"value": ns1 / (single_ms / 1e3), "unit": METRIC,
                                           "sample": f"first {ns1} scenes, one launch each"}
     del singles
 

@@ -88,6 +88,9 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.dense_max = c.sparse_max_bodies;
     e.warp_max_contacts = c.warp_max_contacts;
     e.warp_max_bodies = c.warp_max_bodies;
+    e.mixed = c.precision == PDC_PRECISION_MIXED;
+    e.inner_rtol = c.mixed_inner_rtol;
+    e.max_outer = 30;
     e.rtol_direct = c.pcg_rtol_direct;
     e.max_direct = c.pcg_max_direct;
     e.rtol_iter = c.pcg_rtol_iter;
@@ -154,6 +157,13 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->sf = D(3 * nc);
     P->X = D(3 * nc);
     P->W = D(6 * nc);
+    P->Wf = A.take<float>(6 * nc);
+    P->Xf = A.take<float>(3 * nc);
+    P->rF = A.take<float>(6 * nb);
+    P->zF = A.take<float>(6 * nb);
+    P->pF = A.take<float>(6 * nb);
+    P->eF = A.take<float>(6 * nb);
+    P->pinvf = A.take<float>(21 * nb);
     P->didx = I(nb);
     P->dbody = I(nb);
     P->order_cta = I(ns);

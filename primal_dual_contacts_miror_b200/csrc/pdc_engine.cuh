@@ -36,6 +36,9 @@ struct EngineCfg {
     int dense_max;  // direct branch: sparse Cholesky up to this many active bodies (<= kSparseMax)
     int warp_max_contacts;  // scenes up to this size are solved by one warp
     int warp_max_bodies;
+    int mixed;             // FP32 inner PCG + FP64 iterative refinement
+    double inner_rtol;     // FP32 inner solve relative residual
+    int max_outer;         // refinement steps before giving up
     double rtol_direct;
     int max_direct;
     double rtol_iter;
@@ -104,6 +107,14 @@ struct BatchPtrs {
     double* sf;     // 3
     double* X;      // 3 world vector gathered by bodies
     double* W;      // 6 R K^-1 R^T packed (xx,yy,zz,xy,xz,yz)
+    // mixed precision (FP32 inner PCG): per-contact W and X, per-body vectors
+    float* Wf;     // 6 per contact
+    float* Xf;     // 3 per contact
+    float* rF;     // 6 per body
+    float* zF;
+    float* pF;
+    float* eF;
+    float* pinvf;  // 21 per body
     int* didx;   // dense row-block of each active body
     int* dbody;  // body of each dense row-block (scene-relative slots)
     // per-team sparse-factorisation scratch (see SceneSolver::sparse_ws)
@@ -346,7 +357,7 @@ class SceneSolver {
         cs = csv;
         // sparse direct solve for scenes on the direct branch (the SimplicialLDLT
         // analogue, :385-394): compact node numbering + symbolic factorisation
-        dense_mode = B.dense != nullptr && n_local < C.direct_threshold && C.dense_max > 0 &&
+        dense_mode = !C.mixed && B.dense != nullptr && n_local < C.direct_threshold && C.dense_max > 0 &&
                      n_active <= C.dense_max && n_active > 0 && C.dense_max <= kSparseMax;
         if (dense_mode) {
             T.scan(nb, 0, [&](int b) { return active(b0 + b) ? 1 : 0; },
@@ -579,6 +590,8 @@ class SceneSolver {
                 B.ktInv[3 * gc + 2] = t11;
                 const Frame R = ld_frame(B.frame + 9 * gc);
                 frame_sandwich(R, kni, t00, t01, t11, B.W + 6 * gc);
+                if (C.mixed)
+                    for (int q = 0; q < 6; ++q) B.Wf[6 * gc + q] = (float)B.W[6 * gc + q];
                 const d3 ks = d3{sf0 * kni, t00 * sf1 + t01 * sf2, t01 * sf1 + t11 * sf2};
                 st3(B.X + 3 * gc, from_frame(R, ks));
             }
@@ -637,6 +650,8 @@ class SceneSolver {
                         for (int q = 0; q < 21; ++q) Pi[q] = 0;
                         for (int r = 0; r < 6; ++r) Pi[pk(r, r)] = 1.0 / P[pk(r, r)];
                     }
+                    if (C.mixed)
+                        for (int q = 0; q < 21; ++q) B.pinvf[21 * gb + q] = (float)Pi[q];
                 }
                 for (int r = 0; r < 6; ++r) rr[1] += rb[r] * rb[r];
             }
@@ -653,6 +668,11 @@ class SceneSolver {
             bool lin_bad = false;
             if (dense_mode) {
                 lin_bad = !dense_solve();
+            } else if (C.mixed) {
+                bool conv = true;
+                lin_bad = !mixed_solve(eps, bnorm, rtol, iters, conv);
+                pcg_total += iters;
+                iters = conv ? 0 : maxit;  // the Hu rule sees a capped solve as maxCGIt
             } else {
             if (!direct) {  // AMGCL starts from the previous du (:406-415)
                 spmv_to_X(B.du, nullptr, 0.0);
@@ -1227,6 +1247,184 @@ class SceneSolver {
         (void)n;
         T.sync();
         return !bad;
+    }
+
+    // ------------------------------------------------ mixed precision solve
+    // FP64 iterative refinement of A du = rhs around an FP32 block-Jacobi PCG:
+    // r = rhs - A du in FP64 (matrix-free, FP64 W), e = A^-1 r approximately in
+    // FP32 (FP32 W, X, vectors, preconditioner, FP32 accumulation), du += e.
+    // Returns false on a non-finite residual; conv = refinement reached rtol.
+    __device__ bool mixed_solve(double eps, double bnorm, double rtol, int& inner_total, bool& conv) {
+        inner_total = 0;
+        conv = true;
+        for (int b = tid; b < nb; b += nt) {
+            const int gb = b0 + b;
+            if (!active(gb)) continue;
+            for (int r = 0; r < 6; ++r) {
+                B.du[6 * gb + r] = 0;
+                B.r[6 * gb + r] = B.rhs[6 * gb + r];
+            }
+        }
+        T.sync();
+        if (bnorm == 0) return true;
+        double res = 1.0;
+        const float epsf = (float)eps;
+        for (int outer = 0;; ++outer) {
+            if (!(res >= rtol)) break;
+            if (outer >= C.max_outer) {
+                conv = false;
+                break;
+            }
+            // inner FP32 PCG on A e = r, e0 = 0
+            double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                float r6[6], z6[6];
+                for (int q = 0; q < 6; ++q) r6[q] = (float)B.r[6 * gb + q];
+                prec_f(gb, r6, z6);
+                for (int q = 0; q < 6; ++q) {
+                    B.rF[6 * gb + q] = r6[q];
+                    B.zF[6 * gb + q] = z6[q];
+                    B.pF[6 * gb + q] = 0.f;
+                    B.eF[6 * gb + q] = 0.f;
+                    s2[0] += (double)(r6[q] * z6[q]);
+                    s2[1] += (double)(r6[q] * r6[q]);
+                }
+            }
+            T.sum(s2);
+            float rz = (float)s2[0];
+            const double r0 = sqrt(s2[1]);
+            float beta = 0.f;
+            for (int it = 0; it < C.max_direct && r0 > 0; ++it) {
+                spmv_to_Xf(beta);
+                T.sync();
+                double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int b = tid; b < nb; b += nt) {
+                    const int gb = b0 + b;
+                    if (!active(gb)) continue;
+                    float pn[6], q6[6];
+                    for (int q = 0; q < 6; ++q) {
+                        pn[q] = __fadd_rn(B.zF[6 * gb + q], __fmul_rn(beta, B.pF[6 * gb + q]));
+                        B.pF[6 * gb + q] = pn[q];
+                    }
+                    spmv_body_f(gb, pn, epsf, q6);
+                    float acc = 0.f;
+                    for (int q = 0; q < 6; ++q) {
+                        acc += pn[q] * q6[q];
+                        B.zF[6 * gb + q] = q6[q];
+                    }
+                    s3[0] += (double)acc;
+                }
+                T.sum(s3);
+                const float alpha = rz / (float)s3[0];
+                double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int b = tid; b < nb; b += nt) {
+                    const int gb = b0 + b;
+                    if (!active(gb)) continue;
+                    float r6[6], z6[6];
+                    for (int q = 0; q < 6; ++q) {
+                        B.eF[6 * gb + q] += alpha * B.pF[6 * gb + q];
+                        r6[q] = B.rF[6 * gb + q] - alpha * B.zF[6 * gb + q];
+                        B.rF[6 * gb + q] = r6[q];
+                    }
+                    prec_f(gb, r6, z6);
+                    float a0 = 0.f, a1 = 0.f;
+                    for (int q = 0; q < 6; ++q) {
+                        B.zF[6 * gb + q] = z6[q];
+                        a0 += r6[q] * r6[q];
+                        a1 += r6[q] * z6[q];
+                    }
+                    s4[0] += (double)a0;
+                    s4[1] += (double)a1;
+                }
+                T.sum(s4);
+                ++inner_total;
+                if (!(sqrt(s4[0]) >= C.inner_rtol * r0)) break;
+                beta = (float)s4[1] / rz;
+                rz = (float)s4[1];
+            }
+            // du += e; FP64 residual r = rhs - A du
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                for (int q = 0; q < 6; ++q) B.du[6 * gb + q] += (double)B.eF[6 * gb + q];
+            }
+            T.sync();
+            spmv_to_X(B.du, nullptr, 0.0);
+            T.sync();
+            double s5[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int b = tid; b < nb; b += nt) {
+                const int gb = b0 + b;
+                if (!active(gb)) continue;
+                double q6[6];
+                spmv_body(gb, B.du + 6 * gb, eps, q6);
+                for (int q = 0; q < 6; ++q) {
+                    const double rv = B.rhs[6 * gb + q] - q6[q];
+                    B.r[6 * gb + q] = rv;
+                    s5[0] += rv * rv;
+                }
+            }
+            T.sum(s5);
+            res = sqrt(s5[0]) / bnorm;
+            if (!isfinite(res)) return false;
+        }
+        return true;
+    }
+    // FP32 versions of the matrix-free product and the preconditioner
+    __device__ __forceinline__ void spmv_to_Xf(float beta) const {
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            float pv[2][3];
+            for (int j = 0; j < 2; ++j) {
+                const int gb = b0 + B.cbody[2 * gc + j];
+                if (B.is_static[gb]) {
+                    pv[j][0] = pv[j][1] = pv[j][2] = 0.f;
+                    continue;
+                }
+                float pn[6];
+                for (int q = 0; q < 6; ++q) pn[q] = __fadd_rn(B.zF[6 * gb + q], __fmul_rn(beta, B.pF[6 * gb + q]));
+                const float cx = (float)B.arm[6 * gc + 3 * j], cy = (float)B.arm[6 * gc + 3 * j + 1],
+                            cz = (float)B.arm[6 * gc + 3 * j + 2];
+                pv[j][0] = pn[0] + (pn[4] * cz - pn[5] * cy);
+                pv[j][1] = pn[1] + (pn[5] * cx - pn[3] * cz);
+                pv[j][2] = pn[2] + (pn[3] * cy - pn[4] * cx);
+            }
+            const float* W = B.Wf + 6 * gc;
+            const float d0 = pv[1][0] - pv[0][0], d1 = pv[1][1] - pv[0][1], d2 = pv[1][2] - pv[0][2];
+            B.Xf[3 * gc] = W[0] * d0 + W[3] * d1 + W[4] * d2;
+            B.Xf[3 * gc + 1] = W[3] * d0 + W[1] * d1 + W[5] * d2;
+            B.Xf[3 * gc + 2] = W[4] * d0 + W[5] * d1 + W[2] * d2;
+        }
+    }
+    __device__ __forceinline__ void spmv_body_f(int gb, const float* x6, float epsf, float* q6) const {
+        const float icm = (float)(1.0 / cm);
+        const float m = (float)B.mass[gb] * icm;
+        const double* I = B.inertia + 6 * gb;
+        const float Ixx = (float)I[0] * icm, Iyy = (float)I[1] * icm, Izz = (float)I[2] * icm;
+        const float Ixy = (float)I[3] * icm, Ixz = (float)I[4] * icm, Iyz = (float)I[5] * icm;
+        float a[6] = {m * x6[0], m * x6[1], m * x6[2], Ixx * x6[3] + Ixy * x6[4] + Ixz * x6[5],
+                      Ixy * x6[3] + Iyy * x6[4] + Iyz * x6[5], Ixz * x6[3] + Iyz * x6[4] + Izz * x6[5]};
+        const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+        for (int k = 0; k < n; ++k) {
+            const int e = B.inc[st + k];
+            const int gc = e >> 1, side = e & 1;
+            const float sg = side ? 1.f : -1.f;
+            const float x = sg * B.Xf[3 * gc], y = sg * B.Xf[3 * gc + 1], z = sg * B.Xf[3 * gc + 2];
+            const float cx = (float)B.arm[6 * gc + 3 * side], cy = (float)B.arm[6 * gc + 3 * side + 1],
+                        cz = (float)B.arm[6 * gc + 3 * side + 2];
+            a[0] += x; a[1] += y; a[2] += z;
+            a[3] += cy * z - cz * y; a[4] += cz * x - cx * z; a[5] += cx * y - cy * x;
+        }
+        for (int q = 0; q < 6; ++q) q6[q] = a[q] + epsf * x6[q];
+    }
+    __device__ __forceinline__ void prec_f(int gb, const float* r6, float* z6) const {
+        const float* Pi = B.pinvf + 21 * gb;
+        for (int a = 0; a < 6; ++a) {
+            float s = 0.f;
+            for (int c = 0; c < 6; ++c) s += Pi[pk(a, c)] * r6[c];
+            z6[a] = s;
+        }
     }
 
     // X = W (v1p - v0p) of direction vec (or of z + beta*vec when zvec != null),
