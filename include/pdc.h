@@ -51,7 +51,8 @@ enum pdc_status {
     PDC_ECUDA = 2,    /* a CUDA runtime call failed */
     PDC_ENOMEM = 3,   /* device allocation failed */
     PDC_ETIMEOUT = 4, /* a bounded device wait ran out */
-    PDC_ENODEV = 5    /* no CUDA device / extension unusable */
+    PDC_ENODEV = 5,   /* no CUDA device / extension unusable */
+    PDC_EBUSY = 6     /* serving: no free slot or pool range right now */
 };
 
 /* Per-scene convergence status: returned as data, never as an error, the way the
@@ -277,6 +278,31 @@ int pdc_world_contacts(pdc_world* w, int32_t* counts, int32_t* body, double* fra
                        double* depth, double* pos, double* local_force);
 /* Per-scene solver statistics of the last step and dropped contact points. */
 int pdc_world_stats(pdc_world* w, pdc_stats* stats, int32_t* overflow);
+
+/* ------------------------------------------------------------------------
+ * Serving: continuous batching of scene requests (no counterpart in the
+ * reference, which runs one scene per process).  Fixed device pools of bodies
+ * (max_bodies) and contact slots (contacts_per_body per body + 16 per scene) and
+ * max_scenes scene slots are allocated once; scenes are admitted between ticks
+ * into free slots and pool ranges, every tick advances all admitted scenes by one
+ * step (the world's captured step graph), and a scene whose horizon is reached is
+ * frozen until its final state is taken.  A scene's result does not depend on
+ * which other scenes share its ticks. */
+typedef struct pdc_server pdc_server;
+
+int pdc_server_create(const pdc_config* cfg, double dt, const double gravity[3], int32_t max_scenes,
+                      int64_t max_bodies, int32_t contacts_per_body, pdc_server** out);
+void pdc_server_destroy(pdc_server* v);
+/* Admit one scene for `horizon` steps: PDC_EBUSY when no slot or range is free. */
+int pdc_server_admit(pdc_server* v, const pdc_shapes_soa* scene, int32_t horizon, int32_t* slot_out);
+/* Enqueue one step of every running scene on `stream` (NULL = legacy default stream). */
+int pdc_server_tick(pdc_server* v, void* stream);
+/* Slots that reached their horizon since the last poll (up to max_slots). */
+int pdc_server_poll(pdc_server* v, int32_t* slots, int32_t max_slots, int32_t* n_out);
+/* Copy a finished scene's final state out and free its slot and ranges. */
+int pdc_server_take(pdc_server* v, int32_t slot, double* pos, double* quat, double* vel, double* ang_vel);
+/* Running scenes and pool use. */
+int pdc_server_info(pdc_server* v, int32_t* running, int64_t* bodies_used, int64_t* contacts_used);
 
 /* Wait for the handle's outstanding work (bounded: PDC_ETIMEOUT after timeout_ms). */
 int pdc_sync(pdc_solver* s, int32_t timeout_ms);

@@ -9,9 +9,9 @@ import numpy as np
 
 PDC_ABI_VERSION = 1
 
-PDC_OK, PDC_EINVAL, PDC_ECUDA, PDC_ENOMEM, PDC_ETIMEOUT, PDC_ENODEV = range(6)
+PDC_OK, PDC_EINVAL, PDC_ECUDA, PDC_ENOMEM, PDC_ETIMEOUT, PDC_ENODEV, PDC_EBUSY = range(7)
 STATUS_NAMES = {0: "PDC_OK", 1: "PDC_EINVAL", 2: "PDC_ECUDA", 3: "PDC_ENOMEM",
-                4: "PDC_ETIMEOUT", 5: "PDC_ENODEV"}
+                4: "PDC_ETIMEOUT", 5: "PDC_ENODEV", 6: "PDC_EBUSY"}
 
 PDC_SCENE_OK = 0
 PDC_SCENE_MAX_ITER = 1

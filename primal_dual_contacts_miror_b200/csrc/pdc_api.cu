@@ -665,3 +665,4 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
 }
 
 #include "pdc_world.cuh"
+#include "pdc_server.cuh"

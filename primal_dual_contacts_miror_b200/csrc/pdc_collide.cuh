@@ -20,8 +20,10 @@ enum { SHAPE_BOX = 0, SHAPE_SPHERE = 1, SHAPE_PLANE = 2 };
 
 struct WorldPtrs {
     int n_scenes;
-    const int* body_off;      // [ns+1]
-    const int* contact_cap;   // [ns+1] contact capacity offsets
+    const int* body_off;      // [ns+1] (or per-slot starts when body_cnt is set)
+    const int* contact_cap;   // [ns+1] contact capacity offsets (or per-slot starts)
+    const int* body_cnt;      // optional [ns]: bodies of each slot (serving)
+    const int* cap_cnt;       // optional [ns]: contact capacity of each slot
     const double* dt;         // [ns]
     const double* grav;       // [ns][3]
     // shapes / state

@@ -53,6 +53,7 @@ struct BatchPtrs {
     const int* __restrict__ body_off;
     const int* __restrict__ contact_off;
     const int* __restrict__ contact_cnt;  // optional: contacts used in each slice (else the slice size)
+    const int* __restrict__ body_cnt;     // optional: bodies of each scene (else the slice size)
     const double* __restrict__ dt;
     const double* __restrict__ grav;
     // bodies (inputs)
@@ -181,7 +182,7 @@ class SceneSolver {
         : B(b), C(c), T(t), s(scene) {
         if (B.body_off) {
             b0 = B.body_off[s];
-            nb = B.body_off[s + 1] - b0;
+            nb = B.body_cnt ? B.body_cnt[s] : B.body_off[s + 1] - b0;
             c0 = B.contact_off[s];
             nc = B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - c0;
             dt = B.dt[s];
@@ -1659,7 +1660,7 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
     __syncthreads();
     auto size_of = [&](int s, int& nb, int& nc) {
         if (B.body_off) {
-            nb = B.body_off[s + 1] - B.body_off[s];
+            nb = B.body_cnt ? B.body_cnt[s] : B.body_off[s + 1] - B.body_off[s];
             nc = B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - B.contact_off[s];
         } else {
             nb = B.single_nb;

@@ -10,8 +10,10 @@
 namespace pdc {
 
 // World-frame inertia R I0 R^T and its inverse (RigidObjectBase.cpp:106-119).
-__global__ void prepare_bodies_kernel(const __grid_constant__ WorldPtrs W, int nb) {
+__global__ void prepare_bodies_kernel(const __grid_constant__ WorldPtrs W, const int* __restrict__ body_scene,
+                                      int nb) {
     for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < nb; gb += gridDim.x * blockDim.x) {
+        if (body_scene[gb] < 0) continue;  // free pool entry (serving)
         double R[9];
         quat_to_R(W.quat + 4 * gb, R);
         const double* I0 = W.inertia0 + 3 * gb;
@@ -39,8 +41,8 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ Wo
     __shared__ int s_off[257];
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int s = blockIdx.x; s < W.n_scenes; s += gridDim.x) {
-        const int b0 = W.body_off[s], nb = W.body_off[s + 1] - b0;
-        const int cap0 = W.contact_cap[s], cap = W.contact_cap[s + 1] - cap0;
+        const int b0 = W.body_off[s], nb = W.body_cnt ? W.body_cnt[s] : W.body_off[s + 1] - b0;
+        const int cap0 = W.contact_cap[s], cap = W.cap_cnt ? W.cap_cnt[s] : W.contact_cap[s + 1] - cap0;
         const long long npairs = (long long)nb * (nb - 1) / 2;
         const long long chunk = (npairs + nt - 1) / nt;
         const long long p0 = tid * chunk, p1 = min(npairs, p0 + chunk);
@@ -116,7 +118,9 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ Wo
 // (static bodies move with their prescribed velocity).
 __global__ void integrate_kernel(const __grid_constant__ WorldPtrs W, const int* __restrict__ body_scene, int nb) {
     for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < nb; gb += gridDim.x * blockDim.x) {
-        const double dt = W.dt[body_scene[gb]];
+        const int sc = body_scene[gb];
+        if (sc < 0) continue;  // free pool entry (serving)
+        const double dt = W.dt[sc];
         d3 v = ld3(W.vel + 3 * gb), w = ld3(W.ang + 3 * gb);
         if (!W.is_static[gb]) {
             w = add3(w, ld3(W.dang + 3 * gb));
@@ -169,7 +173,7 @@ struct pdc_world {
 static int world_enqueue_step(pdc_world* w, cudaStream_t st) {
     pdc_solver* s = w->solver;
     const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
-    pdc::prepare_bodies_kernel<<<gb, 256, 0, st>>>(w->W, w->nb);
+    pdc::prepare_bodies_kernel<<<gb, 256, 0, st>>>(w->W, w->body_scene, w->nb);
     CK(cudaGetLastError(), "launch prepare_bodies_kernel");
     const int gc = std::max(1, std::min(w->ns, s->num_sms * 4));
     pdc::collide_kernel<<<gc, 256, 0, st>>>(w->W);
@@ -229,6 +233,8 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
         a.reset();
         pdc::WorldPtrs& W = w->W;
         W.n_scenes = n_scenes;
+        W.body_cnt = nullptr;
+        W.cap_cnt = nullptr;
         W.body_off = a.take<int>(ns + 1);
         W.contact_cap = a.take<int>(ns + 1);
         W.dt = a.take<double>(ns);
@@ -365,7 +371,7 @@ extern "C" int pdc_world_collide(pdc_world* w) {
     pdc_solver* s = w->solver;
     CK(cudaSetDevice(s->device), "cudaSetDevice");
     const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
-    pdc::prepare_bodies_kernel<<<gb, 256, 0, w->stream>>>(w->W, w->nb);
+    pdc::prepare_bodies_kernel<<<gb, 256, 0, w->stream>>>(w->W, w->body_scene, w->nb);
     CK(cudaGetLastError(), "launch prepare_bodies_kernel");
     pdc::collide_kernel<<<std::max(1, std::min(w->ns, s->num_sms * 4)), 256, 0, w->stream>>>(w->W);
     CK(cudaGetLastError(), "launch collide_kernel");

@@ -209,6 +209,76 @@ class World:
             pass
 
 
+class Server:
+    """Continuous batching of scene requests (pdc_server_*)."""
+
+    def __init__(self, max_scenes, max_bodies, dt=0.01, gravity=(0.0, 0.0, -9.81), contacts_per_body=16, cfg=None,
+                 **overrides):
+        self.lib = load()
+        _bind_world(self.lib)
+        self.cfg = cfg if cfg is not None else abi.default_config(**overrides)
+        g = (C.c_double * 3)(*gravity)
+        h = C.c_void_p()
+        rc = self.lib.pdc_server_create(C.byref(self.cfg), dt, g, max_scenes, max_bodies, contacts_per_body,
+                                        C.byref(h))
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+        self.h = h
+        self.sizes = {}
+
+    def _err(self, rc):
+        raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+
+    def admit(self, scene, horizon):
+        """Admit one shape scene (dict of arrays) for `horizon` steps; returns the
+        slot, or None when the server is full right now (PDC_EBUSY)."""
+        sb = abi.ShapeBatch([scene], 0.0, (0.0, 0.0, 0.0))
+        slot = C.c_int32()
+        rc = self.lib.pdc_server_admit(self.h, C.byref(sb.struct()), horizon, C.byref(slot))
+        if rc == abi.PDC_EBUSY:
+            return None
+        if rc != abi.PDC_OK:
+            self._err(rc)
+        self.sizes[slot.value] = sb.n
+        return slot.value
+
+    def tick(self, stream=None):
+        rc = self.lib.pdc_server_tick(self.h, C.c_void_p(stream or 0))
+        if rc != abi.PDC_OK:
+            self._err(rc)
+
+    def poll(self, max_slots=65536):
+        out = np.zeros(max_slots, np.int32)
+        n = C.c_int32()
+        self.lib.pdc_server_poll(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)), max_slots, C.byref(n))
+        return out[: n.value].tolist()
+
+    def take(self, slot):
+        n = self.sizes.pop(slot)
+        pos, quat, vel, ang = np.zeros((n, 3)), np.zeros((n, 4)), np.zeros((n, 3)), np.zeros((n, 3))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        rc = self.lib.pdc_server_take(self.h, slot, dp(pos), dp(quat), dp(vel), dp(ang))
+        if rc != abi.PDC_OK:
+            self._err(rc)
+        return pos, quat, vel, ang
+
+    def info(self):
+        r, bu, cu = C.c_int32(), C.c_int64(), C.c_int64()
+        self.lib.pdc_server_info(self.h, C.byref(r), C.byref(bu), C.byref(cu))
+        return {"running": r.value, "bodies_used": bu.value, "contacts_used": cu.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pdc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _bind_world(lib):
     if getattr(lib, "_world_bound", False):
         return
@@ -230,6 +300,21 @@ def _bind_world(lib):
     lib.pdc_world_contacts.restype = C.c_int
     lib.pdc_world_stats.argtypes = [vp, C.POINTER(abi.Stats), ip]
     lib.pdc_world_stats.restype = C.c_int
+    lib.pdc_server_create.argtypes = [C.POINTER(abi.Config), C.c_double, dp, C.c_int32, C.c_int64, C.c_int32,
+                                      C.POINTER(vp)]
+    lib.pdc_server_create.restype = C.c_int
+    lib.pdc_server_destroy.argtypes = [vp]
+    lib.pdc_server_destroy.restype = None
+    lib.pdc_server_admit.argtypes = [vp, C.POINTER(abi.Shapes), C.c_int32, ip]
+    lib.pdc_server_admit.restype = C.c_int
+    lib.pdc_server_tick.argtypes = [vp, vp]
+    lib.pdc_server_tick.restype = C.c_int
+    lib.pdc_server_poll.argtypes = [vp, ip, C.c_int32, ip]
+    lib.pdc_server_poll.restype = C.c_int
+    lib.pdc_server_take.argtypes = [vp, C.c_int32, dp, dp, dp, dp]
+    lib.pdc_server_take.restype = C.c_int
+    lib.pdc_server_info.argtypes = [vp, ip, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.pdc_server_info.restype = C.c_int
     lib._world_bound = True
 
 
