@@ -56,6 +56,10 @@ struct pdc_solver {
     double t_total = 0, t_build = 0, t_solve = 0, t_ls = 0;
     long long newton_total = 0, solves = 0;
     unsigned long long* d_timers = nullptr;
+    // grid-wide solve of large scenes (cooperative launch)
+    int grid_blocks = 0;
+    void* d_grid = nullptr;
+    pdc::GridSync gsync;
     int* d_counter = nullptr;
 };
 
@@ -88,6 +92,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.dense_max = c.sparse_max_bodies;
     e.warp_max_contacts = c.warp_max_contacts;
     e.warp_max_bodies = c.warp_max_bodies;
+    e.grid_min_bodies = c.grid_min_bodies;
     e.mixed = c.precision == PDC_PRECISION_MIXED;
     e.inner_rtol = c.mixed_inner_rtol;
     e.max_outer = 30;
@@ -222,6 +227,7 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->warp_max_contacts = 0;  // measured: thread blocks win even for small scenes
     c->warp_max_bodies = 0;
     c->cta_threads = 256;
+    c->grid_min_bodies = 1024;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;
     c->pcg_rtol_iter = 1e-8;
@@ -278,6 +284,26 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         return PDC_ECUDA;
     }
     if (s->blocks_per_sm < 1) s->blocks_per_sm = 1;
+    {  // cooperative grid for large scenes: every block co-resident
+        int bps = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pdc::solve_scene_grid_kernel<256>, 256, 0);
+        s->grid_blocks = std::max(1, bps) * s->num_sms;
+        const size_t bytes = 256 + 2 * (size_t)s->grid_blocks * 8 * sizeof(double) + (s->grid_blocks + 1) * sizeof(int);
+        if (e == cudaSuccess) e = cudaMalloc(&s->d_grid, bytes);
+        if (e == cudaSuccess) e = cudaMemset(s->d_grid, 0, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            g_create_error = std::string("CUDA set-up failed: ") + cudaGetErrorString(e);
+            pdc_destroy(s);
+            return PDC_ECUDA;
+        }
+        char* g = static_cast<char*>(s->d_grid);
+        s->gsync.count = reinterpret_cast<unsigned int*>(g);
+        s->gsync.gen = reinterpret_cast<unsigned int*>(g + 64);
+        s->gsync.err = reinterpret_cast<int*>(g + 128);
+        s->gsync.partials = reinterpret_cast<double*>(g + 256);
+        s->gsync.ipartials = reinterpret_cast<int*>(g + 256 + 2 * (size_t)s->grid_blocks * 8 * sizeof(double));
+    }
     *out = s;
     return PDC_OK;
 }
@@ -289,6 +315,7 @@ extern "C" void pdc_destroy(pdc_solver* s) {
     if (s->arena.base) cudaFree(s->arena.base);
     if (s->d_timers) cudaFree(s->d_timers);
     if (s->d_counter) cudaFree(s->d_counter);
+    if (s->d_grid) cudaFree(s->d_grid);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -304,10 +331,14 @@ extern "C" int pdc_reset(pdc_solver* s) {
     return PDC_OK;
 }
 
-static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st) {
+// Enqueue the planner and the batched solve; then, one cooperative whole-GPU
+// launch per scene in `large` (scenes the planner leaves out when
+// P.grid_large is set).
+static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st, const std::vector<int>* large = nullptr) {
     pdc::BatchPtrs P = P0;
     P.timers = s->d_timers;
     if (P.n_scenes == 0) return PDC_OK;
+    P.grid_large = (large && !large->empty() && s->cfg.grid_min_bodies > 0) ? 1 : 0;
     const int grid = grid_for(s, P.n_scenes);
     pdc::EngineCfg C = engine_cfg(s->cfg);
     pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
@@ -315,7 +346,33 @@ static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st) {
     if (s->threads == 128) pdc::solve_scenes_kernel<128><<<grid, 128, 0, st>>>(P, C);
     else pdc::solve_scenes_kernel<256><<<grid, 256, 0, st>>>(P, C);
     CK(cudaGetLastError(), "launch solve_scenes_kernel");
+    if (P.grid_large) {
+        for (int sc : *large) {
+            CK(cudaMemsetAsync(s->gsync.count, 0, sizeof(unsigned int), st), "reset grid barrier");
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3(s->grid_blocks);
+            lc.blockDim = dim3(256);
+            lc.dynamicSmemBytes = 0;
+            lc.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            lc.attrs = attr;
+            lc.numAttrs = 1;
+            CK(cudaLaunchKernelEx(&lc, pdc::solve_scene_grid_kernel<256>, P, C, sc, s->gsync),
+               "launch solve_scene_grid_kernel");
+        }
+    }
     return PDC_OK;
+}
+
+// Scenes of a host-described batch that get the whole GPU.
+static std::vector<int> large_scenes(const pdc_solver* s, int ns, const int* body_offsets) {
+    std::vector<int> out;
+    if (s->cfg.grid_min_bodies <= 0) return out;
+    for (int k = 0; k < ns; ++k)
+        if (body_offsets[k + 1] - body_offsets[k] >= s->cfg.grid_min_bodies) out.push_back(k);
+    return out;
 }
 
 // Host-array validation shared by pdc_solve and pdc_batch_solve.
@@ -388,7 +445,8 @@ static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_so
     } else {
         P.cmu = nullptr;
     }
-    rc = launch(s, P, st);
+    const std::vector<int> large = large_scenes(s, ns, batch->body_offsets);
+    rc = launch(s, P, st, &large);
     if (rc) return rc;
     if (nb) {
         CK(cudaMemcpyAsync(dvel, P.dvel, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
@@ -397,7 +455,13 @@ static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_so
     if (nc) CK(cudaMemcpyAsync(lforce, P.lforce, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     std::vector<pdc_stats> hst(ns);
     if (ns) CK(cudaMemcpyAsync(hst.data(), P.stats, ns * sizeof(pdc_stats), cudaMemcpyDeviceToHost, st), "D2H");
+    int grid_err = 0;
+    if (!large.empty()) CK(cudaMemcpyAsync(&grid_err, s->gsync.err, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaStreamSynchronize(st), "solve");
+    if (grid_err) {  // a grid barrier timed out: results of the large scenes are invalid
+        CK(cudaMemset(s->gsync.err, 0, sizeof(int)), "reset grid error");
+        return fail(s, PDC_ETIMEOUT, "grid barrier timed out in a whole-GPU scene solve");
+    }
     for (int k = 0; k < ns; ++k) {
         s->newton_total += hst[k].newton_iters;
         if (stats) stats[k] = hst[k];
@@ -502,7 +566,9 @@ extern "C" int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3]
     P.lforce = out->local_force;
     P.stats = nullptr;  // per-scene statistics: use pdc_batch_solve_async
     std::memset(&out->stats, 0, sizeof(out->stats));
-    rc = launch(s, P, static_cast<cudaStream_t>(stream));
+    std::vector<int> large;
+    if (s->cfg.grid_min_bodies > 0 && bodies->n >= s->cfg.grid_min_bodies) large.push_back(0);
+    rc = launch(s, P, static_cast<cudaStream_t>(stream), &large);
     if (rc) return rc;
     s->solves += 1;
     return PDC_OK;

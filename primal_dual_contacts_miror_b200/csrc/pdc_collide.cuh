@@ -24,6 +24,7 @@ struct WorldPtrs {
     const int* contact_cap;   // [ns+1] contact capacity offsets (or per-slot starts)
     const int* body_cnt;      // optional [ns]: bodies of each slot (serving)
     const int* cap_cnt;       // optional [ns]: contact capacity of each slot
+    const uint8_t* skip;      // optional [ns]: scenes collided by the sort-based path
     const double* dt;         // [ns]
     const double* grav;       // [ns][3]
     // shapes / state

@@ -229,6 +229,172 @@ struct WarpTeam {
     }
 };
 
+// Grid-wide team for one large scene: a cooperative launch (all blocks
+// co-resident), a sense-reversing grid barrier whose spin is bounded (on time-out
+// it raises `err`, after which every barrier returns at once so the kernel ends),
+// and reductions through per-block partials read back in a fixed block order
+// (double-buffered, so one barrier per reduction).
+struct GridSync {
+    unsigned int* count;  // arrivals of the current generation
+    unsigned int* gen;    // generation counter
+    int* err;             // set on a barrier time-out
+    double* partials;     // [2][gridDim][8]
+    int* ipartials;       // [gridDim + 1] block sums for scans
+};
+#define PDC_BARRIER_SPIN_LIMIT (1LL << 26)
+
+struct GridTeam {
+    int rank, size, slot;
+    GridSync G;
+    double* s_red;  // shared [8][32] for the in-block stage
+    int* s_int;     // shared [33]
+    int parity;
+    __device__ GridTeam(const GridSync& g, double* red_smem, int* int_smem) {
+        rank = blockIdx.x * blockDim.x + threadIdx.x;
+        size = gridDim.x * blockDim.x;
+        slot = 0;
+        G = g;
+        s_red = red_smem;
+        s_int = int_smem;
+        parity = 0;
+    }
+    __device__ void sync() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile int* err = G.err;
+            if (!*err) {
+                volatile unsigned int* genp = G.gen;
+                const unsigned int g = *genp;
+                __threadfence();
+                const unsigned int arrived = atomicAdd(G.count, 1u);
+                if (arrived == gridDim.x - 1) {
+                    *G.count = 0;
+                    __threadfence();
+                    atomicAdd(G.gen, 1u);
+                } else {
+                    long long spins = 0;
+                    while (*genp == g) {
+                        if (++spins > PDC_BARRIER_SPIN_LIMIT || *err) {
+                            atomicExch(G.err, 1);
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+    template <int N, bool MAX>
+    __device__ __forceinline__ void reduce(double (&v)[N]) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        double* part = G.partials + (size_t)parity * gridDim.x * 8;
+        parity ^= 1;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_down_sync(0xffffffffu, x, o);
+                x = MAX ? dmax(x, y) : x + y;
+            }
+            if (lane == 0) s_red[i * 32 + warp] = x;
+        }
+        __syncthreads();
+        if (warp == 0) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                double x = (lane < nw) ? s_red[i * 32 + lane] : (MAX ? -INFINITY : 0.0);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_down_sync(0xffffffffu, x, o);
+                    x = MAX ? dmax(x, y) : x + y;
+                }
+                if (lane == 0) part[blockIdx.x * 8 + i] = x;
+            }
+        }
+        sync();
+        // every block reduces the partials in the same order: warp 0 strides, then a tree
+        if (warp == 0) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                double x = MAX ? -INFINITY : 0.0;
+                for (int b = lane; b < (int)gridDim.x; b += 32) {
+                    const double y = part[b * 8 + i];
+                    x = MAX ? dmax(x, y) : x + y;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_down_sync(0xffffffffu, x, o);
+                    x = MAX ? dmax(x, y) : x + y;
+                }
+                if (lane == 0) s_red[i * 32] = x;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = s_red[i * 32];
+        __syncthreads();
+    }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) { reduce<N, false>(v); }
+    template <int N>
+    __device__ __forceinline__ void max(double (&v)[N]) { reduce<N, true>(v); }
+    // exclusive scan over n items (items split into contiguous per-block chunks)
+    template <typename Get, typename Put>
+    __device__ void scan(int n, int carry0, Get get, Put put) {
+        const int chunk = (n + gridDim.x - 1) / gridDim.x;
+        const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+        // block sum of the chunk
+        int local = 0;
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) local += get(i);
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((threadIdx.x & 31) == 0) s_int[1 + (threadIdx.x >> 5)] = local;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_int[1 + w];
+            G.ipartials[blockIdx.x] = t;
+        }
+        sync();
+        if (threadIdx.x == 0) {
+            int off = carry0;
+            for (int b = 0; b < (int)blockIdx.x; ++b) off += G.ipartials[b];
+            s_int[0] = off;
+        }
+        __syncthreads();
+        // scan of the chunk, blockDim items at a time
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int base = lo; base < hi; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const int val = (i < hi) ? get(i) : 0;
+            int x = val;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_int[1 + warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                int w = (lane < (int)(blockDim.x >> 5)) ? s_int[1 + lane] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                s_int[1 + lane] = w;
+            }
+            __syncthreads();
+            const int excl = x - val + (warp ? s_int[warp] : 0) + s_int[0];
+            if (i < hi) put(i, excl);
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1) s_int[0] = excl + val;
+            __syncthreads();
+        }
+        sync();
+    }
+};
+
 // 6x6 symmetric positive definite inverse via Cholesky; input/output packed
 // lower triangle, row-major (21 values: (0,0),(1,0),(1,1),(2,0),...).
 __device__ __forceinline__ int pk(int r, int c) { return (r >= c) ? (r * (r + 1) / 2 + c) : (c * (c + 1) / 2 + r); }

@@ -36,6 +36,7 @@ struct EngineCfg {
     int dense_max;  // direct branch: sparse Cholesky up to this many active bodies (<= kSparseMax)
     int warp_max_contacts;  // scenes up to this size are solved by one warp
     int warp_max_bodies;
+    int grid_min_bodies;   // scenes with at least this many bodies get the whole GPU
     int mixed;             // FP32 inner PCG + FP64 iterative refinement
     double inner_rtol;     // FP32 inner solve relative residual
     int max_outer;         // refinement steps before giving up
@@ -47,6 +48,7 @@ struct EngineCfg {
 
 struct BatchPtrs {
     int n_scenes;
+    int grid_large;  // the host launches the grid kernel for scenes >= grid_min_bodies
     // single-scene launch (body_off == nullptr): sizes and step passed by value
     int single_nb, single_nc;
     double single_dt, single_g[3];
@@ -1642,7 +1644,7 @@ class SceneSolver {
         st.char_speed = cs;
         st.n_local_bodies = n_local;
         st.factor_blocks = dense_mode ? sparse_ws().cstart[n_active] : 0;
-        st.team = (T.size == 32) ? 1 : 0;
+        st.team = (T.size == 32) ? 1 : (T.size > (int)blockDim.x ? 2 : 0);
         st.status = status;
     }
 };
@@ -1668,13 +1670,15 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
         }
     };
     auto queue_of = [&](int nb, int nc) {
+        if (B.grid_large && C.grid_min_bodies > 0 && nb >= C.grid_min_bodies) return 2;  // host launches it
         return (nc <= C.warp_max_contacts && nb <= C.warp_max_bodies) ? 1 : 0;
     };
     auto bucket_of = [&](int nc) { return 31 - min(31, 32 - __clz(nc + 1)); };  // large first
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
         int nb, nc;
         size_of(s, nb, nc);
-        atomicAdd(&hist[queue_of(nb, nc)][bucket_of(nc)], 1);
+        const int q = queue_of(nb, nc);
+        if (q < 2) atomicAdd(&hist[q][bucket_of(nc)], 1);
     }
     __syncthreads();
     if (threadIdx.x < 2) {
@@ -1692,6 +1696,7 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
         int nb, nc;
         size_of(s, nb, nc);
         const int q = queue_of(nb, nc);
+        if (q == 2) continue;  // large scene: solved by solve_scene_grid_kernel
         const int pos = atomicAdd(&start[q][bucket_of(nc)], 1);
         (q ? B.order_warp : B.order_cta)[pos] = s;
     }
@@ -1708,7 +1713,7 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
     st.gd_fallbacks = 0;
     st.n_local_bodies = 0;
     st.factor_blocks = 0;
-    st.team = (T.size == 32) ? 1 : 0;
+    st.team = (T.size == 32) ? 1 : (T.size > (int)blockDim.x ? 2 : 0);
     st.exit_err = 0;
     st.kkt_stationarity = 0;
     st.kkt_complementarity = 0;
@@ -1764,6 +1769,17 @@ __global__ void __launch_bounds__(THREADS) solve_scenes_kernel(const __grid_cons
         if (q >= n_warp) break;
         run_scene(B, C, W, B.order_warp[q]);
     }
+}
+
+// One large scene solved by the whole GPU (cooperative launch, grid team).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) solve_scene_grid_kernel(const __grid_constant__ BatchPtrs B,
+                                                                   const __grid_constant__ EngineCfg C, int scene,
+                                                                   GridSync G) {
+    __shared__ double s_red[8 * 32];
+    __shared__ int s_int[33];
+    GridTeam T(G, s_red, s_int);
+    run_scene(B, C, T, scene);
 }
 
 }  // namespace pdc

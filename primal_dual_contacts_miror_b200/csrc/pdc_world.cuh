@@ -5,6 +5,7 @@
 // once in a CUDA graph and replayed.  Included at the end of pdc_api.cu (one
 // translation unit with the solver kernels).
 #pragma once
+#include "pdc_broadphase.cuh"
 #include "pdc_collide.cuh"
 
 namespace pdc {
@@ -41,6 +42,7 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ Wo
     __shared__ int s_off[257];
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int s = blockIdx.x; s < W.n_scenes; s += gridDim.x) {
+        if (W.skip && W.skip[s]) continue;  // large scene: sort-based path
         const int b0 = W.body_off[s], nb = W.body_cnt ? W.body_cnt[s] : W.body_off[s + 1] - b0;
         const int cap0 = W.contact_cap[s], cap = W.cap_cnt ? W.cap_cnt[s] : W.contact_cap[s + 1] - cap0;
         const long long npairs = (long long)nb * (nb - 1) / 2;
@@ -168,9 +170,14 @@ struct pdc_world {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     long long steps = 0;
+    std::vector<int> large;  // scenes solved (and collided) by the whole GPU
+    pdc::LargeCollide L;
+    void* large_mem = nullptr;
 };
 
-static int world_enqueue_step(pdc_world* w, cudaStream_t st) {
+// Contact detection of every scene: one block per ordinary scene, the
+// sort-based path for each large scene.
+static int world_collide(pdc_world* w, cudaStream_t st) {
     pdc_solver* s = w->solver;
     const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
     pdc::prepare_bodies_kernel<<<gb, 256, 0, st>>>(w->W, w->body_scene, w->nb);
@@ -178,7 +185,35 @@ static int world_enqueue_step(pdc_world* w, cudaStream_t st) {
     const int gc = std::max(1, std::min(w->ns, s->num_sms * 4));
     pdc::collide_kernel<<<gc, 256, 0, st>>>(w->W);
     CK(cudaGetLastError(), "launch collide_kernel");
-    int rc = launch(s, w->P, st);
+    pdc::LargeCollide& L = w->L;
+    const int gl = s->num_sms * 8;
+    for (int sc : w->large) {
+        CK(cudaMemsetAsync(L.npairs, 0, 2 * sizeof(int), st), "reset pairs");
+        CK(cudaMemsetAsync(L.pairs, 0xff, L.max_pairs * sizeof(unsigned long long), st), "reset pairs");
+        pdc::large_aabb_kernel<<<gl, 256, 0, st>>>(w->W, L, sc);
+        size_t tb = L.temp_bytes;
+        CK(cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_s, L.val, L.val_s, L.nb_max, 0, 32, st),
+           "sort bodies");
+        pdc::large_sweep_kernel<<<gl, 256, 0, st>>>(w->W, L, sc);
+        tb = L.temp_bytes;
+        CK(cub::DeviceRadixSort::SortKeys(L.temp, tb, L.pairs, L.pairs_s, (int)L.max_pairs, 0, 64, st),
+           "sort pairs");
+        pdc::large_narrow_kernel<<<gl, 256, 0, st>>>(w->W, L, sc, 0);
+        tb = L.temp_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(L.temp, tb, L.cnt, L.off, (int)L.max_pairs, st), "scan");
+        pdc::large_narrow_kernel<<<gl, 256, 0, st>>>(w->W, L, sc, 1);
+        pdc::large_total_kernel<<<1, 1, 0, st>>>(w->W, L, sc);
+        CK(cudaGetLastError(), "launch large collision kernels");
+    }
+    return PDC_OK;
+}
+
+static int world_enqueue_step(pdc_world* w, cudaStream_t st) {
+    pdc_solver* s = w->solver;
+    const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
+    int rc = world_collide(w, st);
+    if (rc) return rc;
+    rc = launch(s, w->P, st, &w->large);
     if (rc) return rc;
     pdc::integrate_kernel<<<gb, 256, 0, st>>>(w->W, w->body_scene, w->nb);
     CK(cudaGetLastError(), "launch integrate_kernel");
@@ -235,6 +270,7 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
         W.n_scenes = n_scenes;
         W.body_cnt = nullptr;
         W.cap_cnt = nullptr;
+        W.skip = nullptr;
         W.body_off = a.take<int>(ns + 1);
         W.contact_cap = a.take<int>(ns + 1);
         W.dt = a.take<double>(ns);
@@ -303,6 +339,56 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
         pdc_world_destroy(w);
         return rc;
     }
+    w->large = large_scenes(s, n_scenes, body_offsets);
+    if (!w->large.empty()) {  // buffers of the sort-based path, sized for the largest large scene
+        pdc::LargeCollide& L = w->L;
+        std::memset(&L, 0, sizeof(L));
+        std::vector<uint8_t> skip(n_scenes, 0);
+        for (int sc : w->large) {
+            skip[sc] = 1;
+            L.nb_max = std::max(L.nb_max, body_offsets[sc + 1] - body_offsets[sc]);
+        }
+        L.max_pairs = std::max(1024LL, 64LL * L.nb_max);
+        size_t t1 = 0, t2 = 0, t3 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, t1, (unsigned int*)nullptr, (unsigned int*)nullptr, (int*)nullptr,
+                                        (int*)nullptr, L.nb_max);
+        cub::DeviceRadixSort::SortKeys(nullptr, t2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                       (int)L.max_pairs);
+        cub::DeviceScan::ExclusiveSum(nullptr, t3, (int*)nullptr, (int*)nullptr, (int)L.max_pairs);
+        L.temp_bytes = std::max(t1, std::max(t2, t3));
+        Arena la;
+        auto carve_large = [&](Arena& a) {
+            a.reset();
+            L.key = a.take<unsigned int>(L.nb_max);
+            L.val = a.take<int>(L.nb_max);
+            L.key_s = a.take<unsigned int>(L.nb_max);
+            L.val_s = a.take<int>(L.nb_max);
+            L.box = a.take<float>(6LL * L.nb_max);
+            L.pairs = a.take<unsigned long long>(L.max_pairs);
+            L.pairs_s = a.take<unsigned long long>(L.max_pairs);
+            L.npairs = a.take<int>(2);
+            L.overflow = L.npairs + 1;
+            L.cnt = a.take<int>(L.max_pairs);
+            L.off = a.take<int>(L.max_pairs);
+            L.temp = a.take<char>(L.temp_bytes);
+            return a.off + 256;
+        };
+        const size_t lneed = carve_large(la);
+        cudaError_t le = cudaMalloc(&w->large_mem, lneed + n_scenes);
+        if (le == cudaSuccess) {
+            la.base = w->large_mem;
+            carve_large(la);
+            uint8_t* d_skip = static_cast<uint8_t*>(w->large_mem) + lneed;
+            le = cudaMemcpy(d_skip, skip.data(), n_scenes, cudaMemcpyHostToDevice);
+            W.skip = d_skip;
+        }
+        if (le != cudaSuccess) {
+            cudaGetLastError();
+            pdc_world_destroy(w);
+            return fail(nullptr, le == cudaErrorMemoryAllocation ? PDC_ENOMEM : PDC_ECUDA,
+                        std::string("large-scene collision buffers: ") + cudaGetErrorString(le));
+        }
+    }
     pdc::BatchPtrs& P = w->P;
     P.n_scenes = n_scenes;
     P.body_off = W.body_off;
@@ -336,6 +422,7 @@ extern "C" void pdc_world_destroy(pdc_world* w) {
     if (w->exec) cudaGraphExecDestroy(w->exec);
     if (w->graph) cudaGraphDestroy(w->graph);
     if (w->mem) cudaFree(w->mem);
+    if (w->large_mem) cudaFree(w->large_mem);
     if (w->stream) cudaStreamDestroy(w->stream);
     pdc_destroy(w->solver);
     delete w;
@@ -370,11 +457,8 @@ extern "C" int pdc_world_collide(pdc_world* w) {
     if (!w) return PDC_EINVAL;
     pdc_solver* s = w->solver;
     CK(cudaSetDevice(s->device), "cudaSetDevice");
-    const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
-    pdc::prepare_bodies_kernel<<<gb, 256, 0, w->stream>>>(w->W, w->body_scene, w->nb);
-    CK(cudaGetLastError(), "launch prepare_bodies_kernel");
-    pdc::collide_kernel<<<std::max(1, std::min(w->ns, s->num_sms * 4)), 256, 0, w->stream>>>(w->W);
-    CK(cudaGetLastError(), "launch collide_kernel");
+    int rc = world_collide(w, w->stream);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(w->stream), "collide");
     return PDC_OK;
 }

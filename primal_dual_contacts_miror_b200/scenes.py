@@ -268,6 +268,49 @@ def box_drop_world(n, rng, half_range=(0.05, 0.2), height=40.0, density=1000.0):
     return sb.build()
 
 
+def ball_pit_world(n, rng, side=4.0, r_range=(0.02, 0.05), speed=0.1, density=1000.0):
+    """The large single-scene workload: n spheres (radius ~ U[r_range], density
+    1000) placed i.i.d. uniform without overlap (rejection against a uniform grid
+    hash) inside an open box of `side` m (ground + 4 walls), velocities
+    ~ N(0, speed^2) per axis, no spin."""
+    sb = ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    sb.add_plane((0.0, 0.0, 0.0), "+x")
+    sb.add_plane((side, 0.0, 0.0), "-x")
+    sb.add_plane((0.0, 0.0, 0.0), "+y")
+    sb.add_plane((0.0, side, 0.0), "-y")
+    cell = 2 * r_range[1]
+    grid = {}
+    placed = 0
+    tries = 0
+    while placed < n and tries < 200 * n:
+        tries += 1
+        r = float(rng.uniform(*r_range))
+        p = rng.uniform(r, side - r, 3)
+        key = tuple((p // cell).astype(int))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q, rq in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                        d = p - q
+                        if d @ d < (r + rq) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        grid.setdefault(key, []).append((p, r))
+        sb.add_sphere(r, tuple(p), density, vel=tuple(rng.normal(0.0, speed, 3)))
+        placed += 1
+    return sb.build()
+
+
 def box_drop_batch(n_scenes, seed, n_min=4, n_max=256, **kw):
     rng = np.random.default_rng(seed)
     ns = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_scenes))).astype(int)

@@ -1,0 +1,103 @@
+"""Large scenes on the whole GPU: the grid team (one cooperative launch per
+scene) against the block team and the oracle, and the sort-based contact
+detection against the per-scene all-pairs path."""
+import numpy as np
+import pytest
+
+import oracle_lib
+from primal_dual_contacts_miror_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b, floor=0.0):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), floor, 1e-300))
+
+
+def test_grid_team_matches_block_team():
+    from primal_dual_contacts_miror_b200 import lib
+
+    sc = scenes.pile_batch(5, seed=91, n_min=12, n_max=60)
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    blk = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=0)).batch_solve(batch)
+    grd = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8)).batch_solve(batch)
+    for k in range(len(sc)):
+        b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
+        c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
+        assert _rel(grd[2][c0:c1], blk[2][c0:c1]) < 1e-9
+        v = np.concatenate([grd[0][b0:b1], grd[1][b0:b1]], 1)
+        bv = np.concatenate([blk[0][b0:b1], blk[1][b0:b1]], 1)
+        assert _rel(v, bv, 0.0981) < 1e-9
+        assert abs(grd[3][k]["newton_iters"] - blk[3][k]["newton_iters"]) <= 1
+
+
+@pytest.mark.parametrize("n_boxes,tol,bar", [(1500, 1e-8, 1e-6), (2100, 1e-6, 1e-4)])
+def test_large_pile_matches_oracle(n_boxes, tol, bar):
+    """1,500 boxes: direct branch (PCG at 1e-13 on the GPU, LDL^T in the oracle),
+    Newton tolerance 1e-8.  2,100 boxes: iterative branch (block-Jacobi CG at
+    1e-8, cap 1000, on both sides) at the default Newton tolerance 1e-6; the
+    inexact CG directions trigger gradient-descent fall-backs on both sides, so
+    the bar there is a small multiple of the Newton tolerance."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    s = scenes.settled_pile(n_boxes, np.random.default_rng(n_boxes), vel_noise=0.01)
+    cfg = abi.default_config(tol=tol)
+    dv, da, lf, st = lib.Solver(cfg).solve(s)
+    odv, oda, olf, ost = oracle_lib.solve(s, cfg=cfg, nthreads=8)
+    v = np.concatenate([dv, da], 1)
+    ov = np.concatenate([odv, oda], 1)
+    assert _rel(v, ov, 0.0981) < bar, (_rel(v, ov, 0.0981), st, ost)
+    assert st["status"] == ost["status"] == 0
+    assert st["team"] == 2
+    assert st["n_local_bodies"] == n_boxes + 1
+    assert st["pcg_iters"] > 0
+
+
+def jumbled_large_scene(rng, n_box=500, n_sph=600, L=1.5, H=1.0):
+    """Boxes (random orientation) and spheres at random, overlapping, in an
+    L x L x H region over a ground plane: every pair kind, many contacts."""
+    sb = scenes.ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    for _ in range(n_box):
+        sb.add_box(tuple(rng.uniform(0.03, 0.08, 3)), tuple(rng.uniform([0, 0, 0.0], [L, L, H])),
+                   quat=tuple(scenes.random_quat(rng)))
+    for _ in range(n_sph):
+        sb.add_sphere(float(rng.uniform(0.03, 0.06)), tuple(rng.uniform([0, 0, 0.0], [L, L, H])))
+    return sb.build()
+
+
+def test_sort_based_collision_matches_all_pairs():
+    """The same 1,101-body scene collided by the per-scene all-pairs kernel
+    (large-scene path off) and by the sort-based path: identical contact lists."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    sc = jumbled_large_scene(np.random.default_rng(4))
+    got = {}
+    for gmin in (1024, 0):
+        w = lib.World(abi.ShapeBatch([sc], 0.002, (0, 0, -9.81)), cfg=abi.default_config(grid_min_bodies=gmin),
+                      contacts_per_body=32)
+        w.collide()
+        got[gmin] = w.contacts()
+        st, ov = w.stats()
+        assert ov[0] == 0
+        w.close()
+    (ca, a), (cb, b) = got[1024], got[0]
+    assert ca[0] == cb[0] and ca[0] > 1000, (ca, cb)
+    for k in ("body", "frame", "arm", "depth", "pos"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_ball_pit_world_steps():
+    from primal_dual_contacts_miror_b200 import lib
+
+    sc = scenes.ball_pit_world(3000, np.random.default_rng(8), side=1.5)
+    w = lib.World(abi.ShapeBatch([sc], 0.002, (0, 0, -9.81)), cfg=abi.default_config(tol=1e-6, mu=0.4))
+    w.step(10)
+    w.sync()
+    pos, quat, vel, ang = w.state()
+    st, ov = w.stats()
+    counts, _ = w.contacts()
+    assert ov[0] == 0 and counts[0] > 0
+    assert np.isfinite(pos).all() and np.isfinite(vel).all()
+    assert pos[5:, 2].min() > -0.01  # nothing fell through the ground
+    w.close()
