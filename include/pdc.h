@@ -96,8 +96,12 @@ typedef struct pdc_config {
     int32_t warp_max_bodies;   /* and bodies are solved by one warp, larger ones by a
                                   whole thread block (0 / 0 = blocks only, the default) */
     int32_t cta_threads;       /* threads per block of the solve kernel: 128 or 256 (256) */
-    int32_t grid_min_bodies;   /* scenes with at least this many bodies are solved by the
-                                  whole GPU, one cooperative launch each (1024; 0 = never) */
+    int32_t grid_min_bodies;   /* scenes with at least this many bodies are large: solved one
+                                  launch each, by a thread-block cluster or the whole GPU
+                                  (1024; 0 = never) */
+    int32_t cluster_max_contacts; /* a large scene with at most this many contacts is solved by
+                                  one thread-block cluster (up to 16 CTAs), above it by the
+                                  whole GPU (cooperative launch) (32768; -1 = never) */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
     int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
     double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */
@@ -137,7 +141,8 @@ typedef struct pdc_stats {
     int32_t gd_fallbacks;   /* gradient-descent fallbacks (:444-467) */
     int32_t n_local_bodies; /* bodies in contact (:96-111) */
     int32_t factor_blocks;  /* off-diagonal 6x6 blocks of the sparse factor (0: PCG) */
-    int32_t team;           /* 0: solved by a thread block, 1: by one warp, 2: by the whole GPU */
+    int32_t team;           /* 0: solved by a thread block, 1: by one warp, 2: by the whole GPU,
+                               3: by a thread-block cluster */
     double exit_err;        /* exitErr at exit (:302-307) */
     double kkt_stationarity;/* max(|ru|/6N_b, |rf|/3N_c) */
     double kkt_complementarity; /* max(|lambda.c|_inf, dual gap) */

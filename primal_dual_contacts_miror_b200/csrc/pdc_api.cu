@@ -58,6 +58,7 @@ struct pdc_solver {
     unsigned long long* d_timers = nullptr;
     // grid-wide solve of large scenes (cooperative launch)
     int grid_blocks = 0;
+    int cluster_size = 0;  // CTAs of the cluster team (0: clusters unavailable)
     void* d_grid = nullptr;
     pdc::GridSync gsync;
     int* d_counter = nullptr;
@@ -93,6 +94,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.warp_max_contacts = c.warp_max_contacts;
     e.warp_max_bodies = c.warp_max_bodies;
     e.grid_min_bodies = c.grid_min_bodies;
+    e.cluster_max_contacts = c.cluster_max_contacts;
     e.mixed = c.precision == PDC_PRECISION_MIXED;
     e.inner_rtol = c.mixed_inner_rtol;
     e.max_outer = 30;
@@ -134,16 +136,20 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->inc_cnt = I(nb);
     P->inc_cur = I(nb);
     P->local = A.take<uint8_t>(nb);
+    P->lbody = I(nb);
     P->u = D(6 * nb);
     P->uold = D(6 * nb);
     P->du = D(6 * nb);
     P->r = D(6 * nb);
     P->z = D(6 * nb);
     P->p = D(6 * nb);
+    P->p2 = D(6 * nb);
+    P->q = D(6 * nb);
     P->rhs = D(6 * nb);
     P->ru = D(6 * nb);
     P->pinv = D(21 * nb);
     P->inc = I(2 * nc);
+    P->inc_o = I(2 * nc);
     P->f = D(3 * nc);
     P->lam = D(2 * nc);
     P->fT = D(3 * nc);
@@ -228,6 +234,7 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->warp_max_bodies = 0;
     c->cta_threads = 256;
     c->grid_min_bodies = 1024;
+    c->cluster_max_contacts = 32768;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;
     c->pcg_rtol_iter = 1e-8;
@@ -304,6 +311,26 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         s->gsync.partials = reinterpret_cast<double*>(g + 256);
         s->gsync.ipartials = reinterpret_cast<int*>(g + 256 + 2 * (size_t)s->grid_blocks * 8 * sizeof(double));
     }
+    // cluster team: the largest cluster (16, 8, 4 or 2 CTAs) the kernel can run
+    cudaFuncSetAttribute(pdc::solve_scene_cluster_kernel<256>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int cs : {16, 8, 4, 2}) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(cs);
+        lc.blockDim = dim3(256);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, pdc::solve_scene_cluster_kernel<256>, &lc) == cudaSuccess && n > 0) {
+            s->cluster_size = cs;
+            break;
+        }
+        cudaGetLastError();
+    }
     *out = s;
     return PDC_OK;
 }
@@ -347,7 +374,24 @@ static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st, cons
     else pdc::solve_scenes_kernel<256><<<grid, 256, 0, st>>>(P, C);
     CK(cudaGetLastError(), "launch solve_scenes_kernel");
     if (P.grid_large) {
+        if (!s->cluster_size) C.cluster_max_contacts = -1;
         for (int sc : *large) {
+            if (s->cluster_size && C.cluster_max_contacts >= 0) {  // returns at once if the scene is too big
+                cudaLaunchConfig_t lc = {};
+                lc.gridDim = dim3(s->cluster_size);
+                lc.blockDim = dim3(256);
+                lc.dynamicSmemBytes = 0;
+                lc.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = s->cluster_size;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                lc.attrs = attr;
+                lc.numAttrs = 1;
+                CK(cudaLaunchKernelEx(&lc, pdc::solve_scene_cluster_kernel<256>, P, C, sc),
+                   "launch solve_scene_cluster_kernel");
+            }
             CK(cudaMemsetAsync(s->gsync.count, 0, sizeof(unsigned int), st), "reset grid barrier");
             cudaLaunchConfig_t lc = {};
             lc.gridDim = dim3(s->grid_blocks);

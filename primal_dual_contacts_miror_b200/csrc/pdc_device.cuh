@@ -1,6 +1,7 @@
 // Device-side building blocks of the B200 contact solver: small 3-vector math,
 // the friction-cone functions, and deterministic block reductions.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -81,12 +82,14 @@ struct BlockReducer {
     double* slots;  // [2][N][32] in shared memory
     int parity;
     __device__ void init(double* s) { slots = s; parity = 0; }
-    __device__ __forceinline__ void sum(double (&v)[N]) {
+    template <int M>
+    __device__ __forceinline__ void sum(double (&v)[M]) {
+        static_assert(M <= N, "reduction wider than the slots");
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         double* b = slots + parity * N * 32;
         parity ^= 1;
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
+        for (int i = 0; i < M; ++i) {
             double x = v[i];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
@@ -94,19 +97,21 @@ struct BlockReducer {
         }
         __syncthreads();
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
+        for (int i = 0; i < M; ++i) {
             double x = (lane < nw) ? b[i * 32 + lane] : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             v[i] = __shfl_sync(0xffffffffu, x, 0);
         }
     }
-    __device__ __forceinline__ void max(double (&v)[N]) {
+    template <int M>
+    __device__ __forceinline__ void max(double (&v)[M]) {
+        static_assert(M <= N, "reduction wider than the slots");
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         double* b = slots + parity * N * 32;
         parity ^= 1;
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
+        for (int i = 0; i < M; ++i) {
             double x = v[i];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_down_sync(0xffffffffu, x, o));
@@ -114,7 +119,7 @@ struct BlockReducer {
         }
         __syncthreads();
 #pragma unroll
-        for (int i = 0; i < N; ++i) {
+        for (int i = 0; i < M; ++i) {
             double x = (lane < nw) ? b[i * 32 + lane] : -INFINITY;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) x = dmax(x, __shfl_down_sync(0xffffffffu, x, o));
@@ -129,6 +134,7 @@ struct BlockReducer {
 // __syncwarp and shuffles only, so a block hosts many independent scenes).
 // Both give every member the bitwise-identical result of each reduction.
 struct CtaTeam {
+    static constexpr int kind = 0;
     int rank, size, slot;
     BlockReducer<8> red;
     int* s_int;  // shared: [0] carry, [1..32] warp partials
@@ -183,6 +189,7 @@ struct CtaTeam {
 };
 
 struct WarpTeam {
+    static constexpr int kind = 1;
     int rank, size, slot;
     __device__ WarpTeam(int slot_) {
         rank = threadIdx.x & 31;
@@ -242,8 +249,10 @@ struct GridSync {
     int* ipartials;       // [gridDim + 1] block sums for scans
 };
 #define PDC_BARRIER_SPIN_LIMIT (1LL << 26)
+#define PDC_BARRIER_WAIT_NS 10000000000ULL  // 10 s
 
 struct GridTeam {
+    static constexpr int kind = 2;
     int rank, size, slot;
     GridSync G;
     double* s_red;  // shared [8][32] for the in-block stage
@@ -258,28 +267,39 @@ struct GridTeam {
         s_int = int_smem;
         parity = 0;
     }
+    // Grid barrier on a counter that only grows (zeroed before the launch): the
+    // k-th barrier is passed once the counter reaches k * gridDim.x.  One
+    // release-atomic per block to arrive, acquire loads to wait; a wait longer
+    // than PDC_BARRIER_WAIT_NS sets the error flag, after which every barrier is
+    // skipped and the kernel runs out its bounded loops.
+    unsigned int epoch = 0;
     __device__ void sync() {
         __syncthreads();
         if (threadIdx.x == 0) {
             volatile int* err = G.err;
+            ++epoch;
             if (!*err) {
-                volatile unsigned int* genp = G.gen;
-                const unsigned int g = *genp;
+                const unsigned int target = epoch * gridDim.x;
+                unsigned int v;
                 __threadfence();
-                const unsigned int arrived = atomicAdd(G.count, 1u);
-                if (arrived == gridDim.x - 1) {
-                    *G.count = 0;
-                    __threadfence();
-                    atomicAdd(G.gen, 1u);
-                } else {
-                    long long spins = 0;
-                    while (*genp == g) {
-                        if (++spins > PDC_BARRIER_SPIN_LIMIT || *err) {
-                            atomicExch(G.err, 1);
-                            break;
-                        }
-                        __nanosleep(32);
+                asm volatile("atom.add.release.gpu.u32 %0, [%1], 1;" : "=r"(v) : "l"(G.count) : "memory");
+                ++v;
+                long long spins = 0;
+                unsigned long long t0 = 0;
+                while ((int)(v - target) < 0) {
+                    ++spins;
+                    if ((spins & 1023) == 1) {
+                        unsigned long long t;
+                        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                        if (spins == 1) t0 = t;
+                        else if (t - t0 > PDC_BARRIER_WAIT_NS) spins = PDC_BARRIER_SPIN_LIMIT + 1;
                     }
+                    if (spins > PDC_BARRIER_SPIN_LIMIT || *err) {
+                        atomicExch(G.err, 1);
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(20);
+                    asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(G.count) : "memory");
                 }
                 __threadfence();
             }
@@ -320,6 +340,7 @@ struct GridTeam {
 #pragma unroll
             for (int i = 0; i < N; ++i) {
                 double x = MAX ? -INFINITY : 0.0;
+#pragma unroll 4
                 for (int b = lane; b < (int)gridDim.x; b += 32) {
                     const double y = part[b * 8 + i];
                     x = MAX ? dmax(x, y) : x + y;
@@ -392,6 +413,144 @@ struct GridTeam {
             __syncthreads();
         }
         sync();
+    }
+};
+
+// A thread-block cluster as one team (up to 16 CTAs on neighbouring SMs): the
+// hardware cluster barrier (barrier.cluster arrive.release / wait.acquire) is
+// about a tenth of the cost of a grid-wide barrier, and reductions exchange the
+// per-CTA partials through distributed shared memory.  Every CTA reads the
+// partials in the same order, so every thread gets the same bits.
+struct ClusterTeam {
+    static constexpr int kind = 3;
+    int rank, size, slot;
+    unsigned int crank, csize;
+    double* s_red;   // shared [8][32]: in-block stage
+    double* s_part;  // shared [2][8]: this CTA's partials, read by every CTA
+    int* s_int;      // shared [33]
+    int* s_ipart;    // shared [1]: this CTA's block sum in scans
+    int parity;
+    __device__ ClusterTeam(double* red_smem, double* part_smem, int* int_smem, int* ipart_smem) {
+        namespace cg = cooperative_groups;
+        cg::cluster_group cl = cg::this_cluster();
+        crank = cl.block_rank();
+        csize = cl.num_blocks();
+        rank = crank * blockDim.x + threadIdx.x;
+        size = csize * blockDim.x;
+        slot = blockIdx.x / csize;
+        s_red = red_smem;
+        s_part = part_smem;
+        s_int = int_smem;
+        s_ipart = ipart_smem;
+        parity = 0;
+    }
+    __device__ __forceinline__ void sync() {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+    template <typename T>
+    __device__ __forceinline__ T* remote(T* p, unsigned int r) const {
+        return cooperative_groups::this_cluster().map_shared_rank(p, r);
+    }
+    template <int N, bool MAX>
+    __device__ __forceinline__ void reduce(double (&v)[N]) {
+        static_assert(N <= 8, "reduction wider than the slots");
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        double* part = s_part + parity * 8;
+        parity ^= 1;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double x = v[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_down_sync(0xffffffffu, x, o);
+                x = MAX ? dmax(x, y) : x + y;
+            }
+            if (lane == 0) s_red[i * 32 + warp] = x;
+        }
+        __syncthreads();
+        if (warp == 0) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                double x = (lane < nw) ? s_red[i * 32 + lane] : (MAX ? -INFINITY : 0.0);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_down_sync(0xffffffffu, x, o);
+                    x = MAX ? dmax(x, y) : x + y;
+                }
+                if (lane == 0) part[i] = x;
+            }
+        }
+        sync();  // partials of every CTA visible cluster-wide
+        if (warp == 0) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                double x = ((unsigned)lane < csize) ? *remote(part + i, lane) : (MAX ? -INFINITY : 0.0);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_down_sync(0xffffffffu, x, o);
+                    x = MAX ? dmax(x, y) : x + y;
+                }
+                if (lane == 0) s_red[i * 32] = x;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = s_red[i * 32];
+        __syncthreads();
+    }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) { reduce<N, false>(v); }
+    template <int N>
+    __device__ __forceinline__ void max(double (&v)[N]) { reduce<N, true>(v); }
+    // exclusive scan over n items (contiguous per-CTA chunks)
+    template <typename Get, typename Put>
+    __device__ void scan(int n, int carry0, Get get, Put put) {
+        const int chunk = (n + (int)csize - 1) / (int)csize;
+        const int lo = min(n, (int)crank * chunk), hi = min(n, lo + chunk);
+        int local = 0;
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) local += get(i);
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((threadIdx.x & 31) == 0) s_int[1 + (threadIdx.x >> 5)] = local;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_int[1 + w];
+            *s_ipart = t;
+        }
+        sync();
+        if (threadIdx.x == 0) {
+            int off = carry0;
+            for (unsigned int b = 0; b < crank; ++b) off += *remote(s_ipart, b);
+            s_int[0] = off;
+        }
+        __syncthreads();
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int base = lo; base < hi; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const int val = (i < hi) ? get(i) : 0;
+            int x = val;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_int[1 + warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                int w = (lane < (int)(blockDim.x >> 5)) ? s_int[1 + lane] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += y;
+                }
+                s_int[1 + lane] = w;
+            }
+            __syncthreads();
+            const int excl = x - val + (warp ? s_int[warp] : 0) + s_int[0];
+            if (i < hi) put(i, excl);
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1) s_int[0] = excl + val;
+            __syncthreads();
+        }
+        sync();  // every CTA is done reading the block sums
     }
 };
 

@@ -36,7 +36,8 @@ struct EngineCfg {
     int dense_max;  // direct branch: sparse Cholesky up to this many active bodies (<= kSparseMax)
     int warp_max_contacts;  // scenes up to this size are solved by one warp
     int warp_max_bodies;
-    int grid_min_bodies;   // scenes with at least this many bodies get the whole GPU
+    int grid_min_bodies;   // scenes with at least this many bodies are large
+    int cluster_max_contacts;  // large scenes up to this many contacts go to a cluster team
     int mixed;             // FP32 inner PCG + FP64 iterative refinement
     double inner_rtol;     // FP32 inner solve relative residual
     int max_outer;         // refinement steps before giving up
@@ -81,17 +82,21 @@ struct BatchPtrs {
     int* inc_cnt;
     int* inc_cur;
     uint8_t* local;
+    int* lbody;    // the scene's local bodies (global index), ascending, in its body slice
     double* u;     // 6
     double* uold;  // 6
     double* du;    // 6
     double* r;     // 6
     double* z;     // 6
     double* p;     // 6
+    double* p2;    // 6: PCG direction of the other parity
+    double* q;     // 6: PCG A p
     double* rhs;   // 6
     double* ru;    // 6
     double* pinv;  // 21
     // per-contact workspace
     int* inc;       // 2 per contact
+    int* inc_o;     // 2 per contact: the incidence's other body (global index), -1 if static
     double* f;      // 3
     double* lam;    // 2
     double* fT;     // 3
@@ -278,6 +283,11 @@ class SceneSolver {
         // exclusive scan of counts -> absolute start in inc[]
         T.scan(nb, 2 * c0, [&](int b) { return B.inc_cnt[b0 + b]; },
                    [&](int b, int excl) { B.inc_start[b0 + b] = excl; });
+        // compact list of the local bodies: every later body phase runs over it
+        T.scan(nb, 0, [&](int b) { return (int)B.local[b0 + b]; },
+               [&](int b, int excl) {
+                   if (B.local[b0 + b]) B.lbody[b0 + excl] = b0 + b;
+               });
         // fill incidence lists (slot order arbitrary, sorted below)
         for (int c = tid; c < nc; c += nt) {
             const int gc = c0 + c;
@@ -341,6 +351,8 @@ class SceneSolver {
             for (int k = 0; k < n; ++k) {
                 const int e = B.inc[st + k];
                 spd = dmax(spd, B.X[3 * (e >> 1) + (e & 1)]);
+                const int go = b0 + B.cbody[2 * (e >> 1) + 1 - (e & 1)];
+                B.inc_o[st + k] = B.is_static[go] ? -1 : go;
             }
             const double m = B.mass[gb];
             const double* I = B.inertia + 6 * gb;
@@ -373,8 +385,8 @@ class SceneSolver {
             dense_mode = sparse_symbolic();
         }
         // velocities (non-dimensional) :203-217
-        for (int b = tid; b < nb; b += nt) {
-            const int gb = b0 + b;
+        for (int i = tid; i < n_local; i += nt) {
+            const int gb = B.lbody[b0 + i];
             if (!B.local[gb]) continue;
             for (int r = 0; r < 3; ++r) {
                 double v = B.vel[3 * gb + r], w = B.ang[3 * gb + r];
@@ -542,8 +554,8 @@ class SceneSolver {
                                  e[1], e[2], e[3]);
             }
             T.sync();
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!B.local[gb]) continue;
                 if (B.is_static[gb]) {
                     for (int r = 0; r < 6; ++r) B.ru[6 * gb + r] = 0;
@@ -600,9 +612,9 @@ class SceneSolver {
             }
             T.sync();
             // rhs = sum getTrans(j) K^-1 sf - ru; block-Jacobi blocks; PCG start
-            double rr[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // r.z, b.b
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            double rr[2] = {0, 0};  // r.z, b.b
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 double gth[6];
                 gather(gb, gth);
@@ -681,9 +693,9 @@ class SceneSolver {
                 spmv_to_X(B.du, nullptr, 0.0);
                 T.sync();
             }
-            double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            double s2[2] = {0, 0};
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 double r6[6];
                 if (direct) {
@@ -711,34 +723,35 @@ class SceneSolver {
                 // zero right-hand side: du = x0 (zero on the direct branch)
             } else if (!(res < rtol)) {
                 for (iters = 0; iters < maxit;) {
-                    // contact phase: p_new = z + beta p for both bodies; X = W dv(p_new)
-                    spmv_to_X(B.p, B.z, beta);
-                    T.sync();
-                    double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    for (int b = tid; b < nb; b += nt) {
-                        const int gb = b0 + b;
+                    // p_new = z + beta p (p double-buffered by parity so that the
+                    // neighbours' previous directions stay readable) and q = A p_new
+                    const double* pp = (iters & 1) ? B.p2 : B.p;
+                    double* pc = (iters & 1) ? B.p : B.p2;
+                    double s3[1] = {0};
+                    for (int i = tid; i < n_local; i += nt) {
+                        const int gb = B.lbody[b0 + i];
                         if (!active(gb)) continue;
                         double pn[6], q6[6];
                         for (int r = 0; r < 6; ++r) {
-                            pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, B.p[6 * gb + r]));
-                            B.p[6 * gb + r] = pn[r];
+                            pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, pp[6 * gb + r]));
+                            pc[6 * gb + r] = pn[r];
                         }
-                        spmv_body(gb, pn, eps, q6);
+                        spmv_body_fused(gb, pn, pp, beta, eps, q6);
                         for (int r = 0; r < 6; ++r) {
                             s3[0] += pn[r] * q6[r];
-                            B.z[6 * gb + r] = q6[r];  // z holds q until the update below
+                            B.q[6 * gb + r] = q6[r];
                         }
                     }
                     T.sum(s3);
                     const double alpha = rz / s3[0];
-                    double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    for (int b = tid; b < nb; b += nt) {
-                        const int gb = b0 + b;
+                    double s4[2] = {0, 0};
+                    for (int i = tid; i < n_local; i += nt) {
+                        const int gb = B.lbody[b0 + i];
                         if (!active(gb)) continue;
                         double r6[6], z6[6];
                         for (int r = 0; r < 6; ++r) {
-                            B.du[6 * gb + r] += alpha * B.p[6 * gb + r];
-                            r6[r] = B.r[6 * gb + r] - alpha * B.z[6 * gb + r];
+                            B.du[6 * gb + r] += alpha * pc[6 * gb + r];
+                            r6[r] = B.r[6 * gb + r] - alpha * B.q[6 * gb + r];
                             B.r[6 * gb + r] = r6[r];
                         }
                         prec(gb, r6, z6);
@@ -761,8 +774,8 @@ class SceneSolver {
             }  // PCG branch
             if (lin_bad) {  // LDLT failure analogue (:390-394): du = 0
                 nonfinite = true;
-                for (int b = tid; b < nb; b += nt) {
-                    const int gb = b0 + b;
+                for (int i = tid; i < n_local; i += nt) {
+                    const int gb = B.lbody[b0 + i];
                     for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = 0;
                 }
             }
@@ -795,8 +808,8 @@ class SceneSolver {
             if (step == 0) {
                 useGD = true;
                 gd_total++;
-                for (int b = tid; b < nb; b += nt) {
-                    const int gb = b0 + b;
+                for (int i = tid; i < n_local; i += nt) {
+                    const int gb = B.lbody[b0 + i];
                     if (!B.local[gb]) continue;
                     for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = -B.ru[6 * gb + r];
                 }
@@ -928,8 +941,8 @@ class SceneSolver {
         for (int q = tid; q < n * kSparseWords; q += nt) S.adj[q] = 0;
         for (int q = tid; q < n; q += nt) S.ipos[q] = -1;
         T.sync();
-        for (int b = tid; b < nb; b += nt) {
-            const int gb = b0 + b;
+        for (int l = tid; l < n_local; l += nt) {
+            const int gb = B.lbody[b0 + l];
             if (!active(gb)) continue;
             const int i = B.didx[gb];
             const int st0 = B.inc_start[gb], cnt = B.inc_cnt[gb];
@@ -1260,8 +1273,8 @@ class SceneSolver {
     __device__ bool mixed_solve(double eps, double bnorm, double rtol, int& inner_total, bool& conv) {
         inner_total = 0;
         conv = true;
-        for (int b = tid; b < nb; b += nt) {
-            const int gb = b0 + b;
+        for (int i = tid; i < n_local; i += nt) {
+            const int gb = B.lbody[b0 + i];
             if (!active(gb)) continue;
             for (int r = 0; r < 6; ++r) {
                 B.du[6 * gb + r] = 0;
@@ -1280,8 +1293,8 @@ class SceneSolver {
             }
             // inner FP32 PCG on A e = r, e0 = 0
             double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 float r6[6], z6[6];
                 for (int q = 0; q < 6; ++q) r6[q] = (float)B.r[6 * gb + q];
@@ -1303,8 +1316,8 @@ class SceneSolver {
                 spmv_to_Xf(beta);
                 T.sync();
                 double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (int b = tid; b < nb; b += nt) {
-                    const int gb = b0 + b;
+                for (int i = tid; i < n_local; i += nt) {
+                    const int gb = B.lbody[b0 + i];
                     if (!active(gb)) continue;
                     float pn[6], q6[6];
                     for (int q = 0; q < 6; ++q) {
@@ -1322,8 +1335,8 @@ class SceneSolver {
                 T.sum(s3);
                 const float alpha = rz / (float)s3[0];
                 double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (int b = tid; b < nb; b += nt) {
-                    const int gb = b0 + b;
+                for (int i = tid; i < n_local; i += nt) {
+                    const int gb = B.lbody[b0 + i];
                     if (!active(gb)) continue;
                     float r6[6], z6[6];
                     for (int q = 0; q < 6; ++q) {
@@ -1348,8 +1361,8 @@ class SceneSolver {
                 rz = (float)s4[1];
             }
             // du += e; FP64 residual r = rhs - A du
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 for (int q = 0; q < 6; ++q) B.du[6 * gb + q] += (double)B.eF[6 * gb + q];
             }
@@ -1357,8 +1370,8 @@ class SceneSolver {
             spmv_to_X(B.du, nullptr, 0.0);
             T.sync();
             double s5[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 double q6[6];
                 spmv_body(gb, B.du + 6 * gb, eps, q6);
@@ -1457,6 +1470,41 @@ class SceneSolver {
         gather(gb, gth);
         for (int r = 0; r < 6; ++r) q6[r] = y[r] + eps * x6[r] + gth[r];
     }
+    // spmv_body of the direction pn = z + beta pp of body gb with each incident
+    // contact's X = W (v1p - v0p) recomputed here (the other body's direction
+    // from z + beta pp) instead of read from a contact phase: the same operations
+    // as spmv_to_X + spmv_body, so the same bits, with no barrier between them.
+    __device__ __forceinline__ void spmv_body_fused(int gb, const double* pn, const double* pp, double beta,
+                                                    double eps, double* q6) const {
+        double y[6];
+        mass_mul(gb, pn, y);
+        const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+#pragma unroll 2
+        for (int k = 0; k < n; ++k) {
+            const int e = B.inc[st + k], go = B.inc_o[st + k];
+            const int gc = e >> 1, side = e & 1;
+            const d3 arm = ld3(B.arm + 6 * gc + 3 * side);
+            const d3 pv_own = point_vel(pn, arm);
+            d3 pv_oth = d3{0, 0, 0};
+            if (go >= 0) {
+                double po[6];
+                for (int r = 0; r < 6; ++r) po[r] = __dadd_rn(B.z[6 * go + r], __dmul_rn(beta, pp[6 * go + r]));
+                pv_oth = point_vel(po, ld3(B.arm + 6 * gc + 3 * (1 - side)));
+            }
+            d3 x = sym_mul(B.W + 6 * gc, side ? sub3(pv_own, pv_oth) : sub3(pv_oth, pv_own));
+            if (!side) x = scl3(-1.0, x);
+            const d3 t = cross3(arm, x);
+            a0 += x.x; a1 += x.y; a2 += x.z;
+            a3 += t.x; a4 += t.y; a5 += t.z;
+        }
+        q6[0] = y[0] + eps * pn[0] + a0;
+        q6[1] = y[1] + eps * pn[1] + a1;
+        q6[2] = y[2] + eps * pn[2] + a2;
+        q6[3] = y[3] + eps * pn[3] + a3;
+        q6[4] = y[4] + eps * pn[4] + a4;
+        q6[5] = y[5] + eps * pn[5] + a5;
+    }
     __device__ __forceinline__ void prec(int gb, const double* r6, double* z6) const {
         const double* Pi = B.pinv + 21 * gb;
         for (int a = 0; a < 6; ++a) {
@@ -1534,8 +1582,8 @@ class SceneSolver {
                 e[6] += (dlin[0] / lI[0]) * rlv[0] + (dlin[1] / lI[1]) * rlv[1];
             }
             T.sync();
-            for (int b = tid; b < nb; b += nt) {
-                const int gb = b0 + b;
+            for (int i = tid; i < n_local; i += nt) {
+                const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
                 double ui[6], ruv[6];
                 trial_u(gb, step, ui);
@@ -1551,8 +1599,8 @@ class SceneSolver {
             const bool acpt = (inErr < sErr) | (sacIn < sacErr);
             if ((acpt && gErr > 0) || (t == maxLS - 1)) {
                 if (acpt) {
-                    for (int b = tid; b < nb; b += nt) {
-                        const int gb = b0 + b;
+                    for (int i = tid; i < n_local; i += nt) {
+                        const int gb = B.lbody[b0 + i];
                         if (!B.local[gb]) continue;
                         double ui[6];
                         trial_u(gb, step, ui);
@@ -1626,8 +1674,8 @@ class SceneSolver {
             for (int k = 0; k < 3; ++k) B.lforce[3 * gc + k] = B.f[3 * gc + k] * cs * cm;
         }
         T.sync();
-        for (int b = tid; b < nb; b += nt) {
-            const int gb = b0 + b;
+        for (int i = tid; i < n_local; i += nt) {
+            const int gb = B.lbody[b0 + i];
             if (!B.local[gb]) continue;
             if (!B.is_static[gb]) body_residual(gb, B.u + 6 * gb, nullptr, e[0]);
             for (int r = 0; r < 3; ++r) {
@@ -1644,7 +1692,7 @@ class SceneSolver {
         st.char_speed = cs;
         st.n_local_bodies = n_local;
         st.factor_blocks = dense_mode ? sparse_ws().cstart[n_active] : 0;
-        st.team = (T.size == 32) ? 1 : (T.size > (int)blockDim.x ? 2 : 0);
+        st.team = Team::kind;
         st.status = status;
     }
 };
@@ -1713,7 +1761,7 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
     st.gd_fallbacks = 0;
     st.n_local_bodies = 0;
     st.factor_blocks = 0;
-    st.team = (T.size == 32) ? 1 : (T.size > (int)blockDim.x ? 2 : 0);
+    st.team = Team::kind;
     st.exit_err = 0;
     st.kkt_stationarity = 0;
     st.kkt_complementarity = 0;
@@ -1771,14 +1819,38 @@ __global__ void __launch_bounds__(THREADS) solve_scenes_kernel(const __grid_cons
     }
 }
 
+// Team of a large scene, decided on the device from its current contact count
+// (the world's counts are only known there): a cluster team up to
+// C.cluster_max_contacts contacts, the whole GPU above.
+__device__ __forceinline__ bool large_on_cluster(const BatchPtrs& B, const EngineCfg& C, int s) {
+    const int nc = B.body_off ? (B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - B.contact_off[s])
+                              : B.single_nc;
+    return nc <= C.cluster_max_contacts;
+}
+
 // One large scene solved by the whole GPU (cooperative launch, grid team).
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) solve_scene_grid_kernel(const __grid_constant__ BatchPtrs B,
                                                                    const __grid_constant__ EngineCfg C, int scene,
                                                                    GridSync G) {
+    if (large_on_cluster(B, C, scene)) return;  // same decision in every block
     __shared__ double s_red[8 * 32];
     __shared__ int s_int[33];
     GridTeam T(G, s_red, s_int);
+    run_scene(B, C, T, scene);
+}
+
+// One large scene of moderate contact count solved by one thread-block cluster.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) solve_scene_cluster_kernel(const __grid_constant__ BatchPtrs B,
+                                                                      const __grid_constant__ EngineCfg C,
+                                                                      int scene) {
+    if (!large_on_cluster(B, C, scene)) return;  // same decision in every block
+    __shared__ double s_red[8 * 32];
+    __shared__ double s_part[2 * 8];
+    __shared__ int s_int[33];
+    __shared__ int s_ipart[1];
+    ClusterTeam T(s_red, s_part, s_int, s_ipart);
     run_scene(B, C, T, scene);
 }
 

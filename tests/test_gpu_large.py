@@ -14,25 +14,40 @@ def _rel(a, b, floor=0.0):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), floor, 1e-300))
 
 
-def test_grid_team_matches_block_team():
+# team kinds in pdc_stats.team, and the cluster_max_contacts that routes a large scene to them
+TEAMS = {"grid": (2, -1), "cluster": (3, 1 << 30)}
+
+
+@pytest.mark.parametrize("team", sorted(TEAMS))
+def test_large_teams_match_block_team(team):
+    """Scenes routed to a large-scene team (grid_min_bodies lowered) against the
+    same scenes on the thread-block team: the sparse direct solve, the PCG and
+    the reductions run on the whole GPU or on one cluster."""
     from primal_dual_contacts_miror_b200 import lib
 
+    kind, cmax = TEAMS[team]
     sc = scenes.pile_batch(5, seed=91, n_min=12, n_max=60)
+    sc.append(scenes.settled_pile(300, np.random.default_rng(3), vel_noise=0.01))  # PCG (> 256 bodies)
     batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
     blk = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=0)).batch_solve(batch)
-    grd = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8)).batch_solve(batch)
+    big = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8, cluster_max_contacts=cmax)).batch_solve(batch)
     for k in range(len(sc)):
         b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
         c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
-        assert _rel(grd[2][c0:c1], blk[2][c0:c1]) < 1e-9
-        v = np.concatenate([grd[0][b0:b1], grd[1][b0:b1]], 1)
+        assert big[3][k]["team"] == kind
+        assert _rel(big[2][c0:c1], blk[2][c0:c1]) < 1e-9
+        v = np.concatenate([big[0][b0:b1], big[1][b0:b1]], 1)
         bv = np.concatenate([blk[0][b0:b1], blk[1][b0:b1]], 1)
         assert _rel(v, bv, 0.0981) < 1e-9
-        assert abs(grd[3][k]["newton_iters"] - blk[3][k]["newton_iters"]) <= 1
+        assert abs(big[3][k]["newton_iters"] - blk[3][k]["newton_iters"]) <= 1
 
 
+_ORACLE = {}
+
+
+@pytest.mark.parametrize("team", sorted(TEAMS))
 @pytest.mark.parametrize("n_boxes,tol,bar", [(1500, 1e-8, 1e-6), (2100, 1e-6, 1e-4)])
-def test_large_pile_matches_oracle(n_boxes, tol, bar):
+def test_large_pile_matches_oracle(n_boxes, tol, bar, team):
     """1,500 boxes: direct branch (PCG at 1e-13 on the GPU, LDL^T in the oracle),
     Newton tolerance 1e-8.  2,100 boxes: iterative branch (block-Jacobi CG at
     1e-8, cap 1000, on both sides) at the default Newton tolerance 1e-6; the
@@ -40,15 +55,18 @@ def test_large_pile_matches_oracle(n_boxes, tol, bar):
     the bar there is a small multiple of the Newton tolerance."""
     from primal_dual_contacts_miror_b200 import lib
 
+    kind, cmax = TEAMS[team]
     s = scenes.settled_pile(n_boxes, np.random.default_rng(n_boxes), vel_noise=0.01)
     cfg = abi.default_config(tol=tol)
-    dv, da, lf, st = lib.Solver(cfg).solve(s)
-    odv, oda, olf, ost = oracle_lib.solve(s, cfg=cfg, nthreads=8)
+    dv, da, lf, st = lib.Solver(abi.default_config(tol=tol, cluster_max_contacts=cmax)).solve(s)
+    if n_boxes not in _ORACLE:
+        _ORACLE[n_boxes] = oracle_lib.solve(s, cfg=cfg, nthreads=8)
+    odv, oda, olf, ost = _ORACLE[n_boxes]
     v = np.concatenate([dv, da], 1)
     ov = np.concatenate([odv, oda], 1)
     assert _rel(v, ov, 0.0981) < bar, (_rel(v, ov, 0.0981), st, ost)
     assert st["status"] == ost["status"] == 0
-    assert st["team"] == 2
+    assert st["team"] == kind
     assert st["n_local_bodies"] == n_boxes + 1
     assert st["pcg_iters"] > 0
 
