@@ -101,7 +101,9 @@ typedef struct pdc_config {
                                   (1024; 0 = never) */
     int32_t cluster_max_contacts; /* a large scene with at most this many contacts is solved by
                                   one thread-block cluster (up to 16 CTAs), above it by the
-                                  whole GPU (cooperative launch) (32768; -1 = never) */
+                                  whole GPU (cooperative launch) (4096; -1 = never) */
+    int32_t pcg_lanes;         /* lanes per body in the PCG product: 1, 2, 4 or 8 (0 = 1 for
+                                  block and warp teams, 4 for the large-scene teams) */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */
     int32_t pcg_max_direct;   /* PCG iteration cap on the direct branch (4000) */
     double pcg_rtol_iter;     /* relative residual of the iterative branch (1e-8, AMGCL's) */

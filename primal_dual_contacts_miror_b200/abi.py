@@ -48,6 +48,7 @@ class Config(C.Structure):
         ("cta_threads", C.c_int32),
         ("grid_min_bodies", C.c_int32),
         ("cluster_max_contacts", C.c_int32),
+        ("pcg_lanes", C.c_int32),
         ("pcg_rtol_direct", C.c_double),
         ("pcg_max_direct", C.c_int32),
         ("pcg_rtol_iter", C.c_double),
@@ -201,7 +202,8 @@ def default_config(**overrides):
     cfg.warp_max_bodies = 0
     cfg.cta_threads = 256
     cfg.grid_min_bodies = 1024
-    cfg.cluster_max_contacts = 32768
+    cfg.cluster_max_contacts = 4096
+    cfg.pcg_lanes = 0
     cfg.pcg_rtol_direct = 1e-13
     cfg.pcg_max_direct = 4000
     cfg.pcg_rtol_iter = 1e-8

@@ -95,6 +95,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.warp_max_bodies = c.warp_max_bodies;
     e.grid_min_bodies = c.grid_min_bodies;
     e.cluster_max_contacts = c.cluster_max_contacts;
+    e.pcg_lanes = c.pcg_lanes;
     e.mixed = c.precision == PDC_PRECISION_MIXED;
     e.inner_rtol = c.mixed_inner_rtol;
     e.max_outer = 30;
@@ -234,7 +235,8 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->warp_max_bodies = 0;
     c->cta_threads = 256;
     c->grid_min_bodies = 1024;
-    c->cluster_max_contacts = 32768;
+    c->cluster_max_contacts = 4096;
+    c->pcg_lanes = 0;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;
     c->pcg_rtol_iter = 1e-8;
@@ -253,6 +255,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
     if (c->precision != PDC_PRECISION_FP64 && c->precision != PDC_PRECISION_MIXED)
         return fail(s, PDC_EINVAL, "unknown precision");
     if (c->pcg_max_direct <= 0 || c->pcg_max_iter <= 0) return fail(s, PDC_EINVAL, "bad PCG caps");
+    if (c->pcg_lanes != 0 && c->pcg_lanes != 1 && c->pcg_lanes != 2 && c->pcg_lanes != 4 && c->pcg_lanes != 8)
+        return fail(s, PDC_EINVAL, "pcg_lanes not in {0, 1, 2, 4, 8}");
     if (c->sparse_max_bodies < 0 || c->sparse_max_bodies > pdc::kSparseMax)
         return fail(s, PDC_EINVAL, "sparse_max_bodies out of [0, 256]");
     return PDC_OK;

@@ -135,6 +135,7 @@ struct BlockReducer {
 // Both give every member the bitwise-identical result of each reduction.
 struct CtaTeam {
     static constexpr int kind = 0;
+    static constexpr int spmv_lanes = 1;  // lanes per body in the PCG product
     int rank, size, slot;
     BlockReducer<8> red;
     int* s_int;  // shared: [0] carry, [1..32] warp partials
@@ -190,6 +191,7 @@ struct CtaTeam {
 
 struct WarpTeam {
     static constexpr int kind = 1;
+    static constexpr int spmv_lanes = 1;  // lanes per body in the PCG product
     int rank, size, slot;
     __device__ WarpTeam(int slot_) {
         rank = threadIdx.x & 31;
@@ -253,6 +255,7 @@ struct GridSync {
 
 struct GridTeam {
     static constexpr int kind = 2;
+    static constexpr int spmv_lanes = 4;  // lanes per body in the PCG product
     int rank, size, slot;
     GridSync G;
     double* s_red;  // shared [8][32] for the in-block stage
@@ -423,6 +426,7 @@ struct GridTeam {
 // partials in the same order, so every thread gets the same bits.
 struct ClusterTeam {
     static constexpr int kind = 3;
+    static constexpr int spmv_lanes = 4;  // lanes per body in the PCG product
     int rank, size, slot;
     unsigned int crank, csize;
     double* s_red;   // shared [8][32]: in-block stage

@@ -38,6 +38,7 @@ struct EngineCfg {
     int warp_max_bodies;
     int grid_min_bodies;   // scenes with at least this many bodies are large
     int cluster_max_contacts;  // large scenes up to this many contacts go to a cluster team
+    int pcg_lanes;             // lanes per body in the PCG product (0: the team's default)
     int mixed;             // FP32 inner PCG + FP64 iterative refinement
     double inner_rtol;     // FP32 inner solve relative residual
     int max_outer;         // refinement steps before giving up
@@ -678,6 +679,7 @@ class SceneSolver {
 
             // ---- linear solve: block-Jacobi PCG (replaces LDLT / AMGCL, :385-427)
             const double rtol = direct ? C.rtol_direct : C.rtol_iter;
+            const int lanes = (C.pcg_lanes > 0 && nt % 32 == 0) ? C.pcg_lanes : Team::spmv_lanes;
             const int maxit = direct ? C.max_direct : C.max_cg;
             int iters = 0;
             bool lin_bad = false;
@@ -728,19 +730,11 @@ class SceneSolver {
                     const double* pp = (iters & 1) ? B.p2 : B.p;
                     double* pc = (iters & 1) ? B.p : B.p2;
                     double s3[1] = {0};
-                    for (int i = tid; i < n_local; i += nt) {
-                        const int gb = B.lbody[b0 + i];
-                        if (!active(gb)) continue;
-                        double pn[6], q6[6];
-                        for (int r = 0; r < 6; ++r) {
-                            pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, pp[6 * gb + r]));
-                            pc[6 * gb + r] = pn[r];
-                        }
-                        spmv_body_fused(gb, pn, pp, beta, eps, q6);
-                        for (int r = 0; r < 6; ++r) {
-                            s3[0] += pn[r] * q6[r];
-                            B.q[6 * gb + r] = q6[r];
-                        }
+                    switch (lanes) {
+                        case 8: pcg_product<8>(pp, pc, beta, eps, s3[0]); break;
+                        case 4: pcg_product<4>(pp, pc, beta, eps, s3[0]); break;
+                        case 2: pcg_product<2>(pp, pc, beta, eps, s3[0]); break;
+                        default: pcg_product<1>(pp, pc, beta, eps, s3[0]); break;
                     }
                     T.sum(s3);
                     const double alpha = rz / s3[0];
@@ -1474,14 +1468,45 @@ class SceneSolver {
     // contact's X = W (v1p - v0p) recomputed here (the other body's direction
     // from z + beta pp) instead of read from a contact phase: the same operations
     // as spmv_to_X + spmv_body, so the same bits, with no barrier between them.
+    // PCG product of every active body: p_new = z + beta pp into pc, q = A p_new,
+    // and this thread's share of p_new . q.  L lanes per body split its
+    // incidences; the loop runs in rounds so every lane of a warp takes the same
+    // trips (the shuffles need the whole warp).
+    template <int L>
+    __device__ __forceinline__ void pcg_product(const double* pp, double* pc, double beta, double eps,
+                                                double& pq) const {
+        const int grp = tid / L, lg = tid - grp * L, ngrp = nt / L;
+        for (int base = 0; base < n_local; base += ngrp) {
+            const int i = base + grp;
+            int gb = -1;
+            if (i < n_local) {
+                gb = B.lbody[b0 + i];
+                if (!active(gb)) gb = -1;
+            }
+            double pn[6], q6[6];
+            if (gb >= 0)
+                for (int r = 0; r < 6; ++r) pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, pp[6 * gb + r]));
+            spmv_body_fused<L>(gb, pn, pp, beta, eps, q6, lg);
+            if (gb >= 0 && lg == 0) {
+                for (int r = 0; r < 6; ++r) {
+                    pc[6 * gb + r] = pn[r];
+                    pq += pn[r] * q6[r];
+                    B.q[6 * gb + r] = q6[r];
+                }
+            }
+        }
+    }
+    // With L > 1, lane lg of the body's group takes incidences lg, lg + L, ...
+    // and a butterfly of shuffles sums the groups' partials (each level adds the
+    // same two values on both lanes, so every lane gets the same bits); gb < 0
+    // (no body for this group) still takes part in the shuffles.
+    template <int L>
     __device__ __forceinline__ void spmv_body_fused(int gb, const double* pn, const double* pp, double beta,
-                                                    double eps, double* q6) const {
-        double y[6];
-        mass_mul(gb, pn, y);
-        const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+                                                    double eps, double* q6, int lg) const {
         double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+        const int st = (gb >= 0) ? B.inc_start[gb] : 0, n = (gb >= 0) ? B.inc_cnt[gb] : 0;
 #pragma unroll 2
-        for (int k = 0; k < n; ++k) {
+        for (int k = lg; k < n; k += L) {
             const int e = B.inc[st + k], go = B.inc_o[st + k];
             const int gc = e >> 1, side = e & 1;
             const d3 arm = ld3(B.arm + 6 * gc + 3 * side);
@@ -1498,6 +1523,20 @@ class SceneSolver {
             a0 += x.x; a1 += x.y; a2 += x.z;
             a3 += t.x; a4 += t.y; a5 += t.z;
         }
+        if constexpr (L > 1) {
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o, L);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o, L);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o, L);
+                a3 += __shfl_xor_sync(0xffffffffu, a3, o, L);
+                a4 += __shfl_xor_sync(0xffffffffu, a4, o, L);
+                a5 += __shfl_xor_sync(0xffffffffu, a5, o, L);
+            }
+        }
+        if (gb < 0) return;
+        double y[6];
+        mass_mul(gb, pn, y);
         q6[0] = y[0] + eps * pn[0] + a0;
         q6[1] = y[1] + eps * pn[1] + a1;
         q6[2] = y[2] + eps * pn[2] + a2;

@@ -42,6 +42,26 @@ def test_large_teams_match_block_team(team):
         assert abs(big[3][k]["newton_iters"] - blk[3][k]["newton_iters"]) <= 1
 
 
+@pytest.mark.parametrize("lanes", [2, 4, 8])
+def test_pcg_lanes_agree(lanes):
+    """The PCG product with several lanes per body (incidences split across
+    lanes, partials combined by shuffles) against one lane per body, on a block
+    team and on the whole GPU: the same solve up to round-off."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    s = scenes.settled_pile(400, np.random.default_rng(5), vel_noise=0.01)
+    for gmin in (0, 8):
+        one = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=gmin, pcg_lanes=1)).solve(s)
+        many = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=gmin, pcg_lanes=lanes,
+                                             cluster_max_contacts=-1)).solve(s)
+        assert one[3]["pcg_iters"] > 0
+        assert _rel(many[2], one[2]) < 1e-9
+        v1 = np.concatenate([one[0], one[1]], 1)
+        vm = np.concatenate([many[0], many[1]], 1)
+        assert _rel(vm, v1, 0.0981) < 1e-9
+        assert abs(many[3]["newton_iters"] - one[3]["newton_iters"]) <= 1
+
+
 _ORACLE = {}
 
 
