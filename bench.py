@@ -210,6 +210,90 @@ def run_world(args, cfg, lib, torch, stream, local, rank, world):
                                                 f"timed after {args.world_settle} steps"}
 
 
+def _solve_timed(lib, cfg, hs, dt, reps=3):
+    """Solve-only time of one contact set through the public API (host arrays)."""
+    s = lib.Solver(cfg)
+    out = s.solve(hs, dt=dt)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = s.solve(hs, dt=dt)
+        ts.append(time.perf_counter() - t0)
+    s.close()
+    return min(ts), out
+
+
+def run_large(args, base_cfg, lib, torch, stream, cpu_cores):
+    """The single large scenes, each as a device world from its initial state:
+    50,000 spheres in an open box (mu 0.4, dt 1/500, all 200 steps) and 2,000
+    boxes dropped in a walled column (per-pair mu ~ U[0.3, 0.8], dt 1/200, the
+    first `pile_steps` of its 1,000 steps).  Steps are collide + solve +
+    integrate CUDA-graph replays timed with events.  The final contact set is
+    then solved alone: FP64 and mixed precision on the GPU, and once by the CPU
+    oracle with all host cores (the velocity errors below are against it)."""
+    out = {}
+    specs = [
+        ("ball_pit_50000", lambda: scenes.ball_pit_world(50000, np.random.default_rng(20241203 + 5 * 10 ** 6)),
+         0.002, args.pit_steps, dict(mu=0.4), 8,
+         "50,000 spheres, r ~ U[0.02, 0.05] m, in a 4x4x4 m open box, v ~ N(0, 0.1^2), mu 0.4, dt 1/500"),
+        ("box_pile_2000", lambda: scenes.box_drop_world(2000, np.random.default_rng(20241203 + 2 * 10 ** 6)),
+         0.005, args.pile_steps, dict(mu_pair_lo=0.3, mu_pair_hi=0.8, mu_pair_seed=20241203), 16,
+         "2,000 boxes, half-extents U[0.05, 0.2] m, dropped in a 10x10x40 m walled column, "
+         "per-pair mu U[0.3, 0.8], dt 1/200"),
+    ]
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    for name, make, dt, steps, kw, cpb, desc in specs:
+        cfg = abi.default_config(**{n: getattr(base_cfg, n) for n, _ in abi.Config._fields_})
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        sc = make()
+        w = lib.World(abi.ShapeBatch([sc], dt, (0.0, 0.0, -9.81)), cfg=cfg, contacts_per_body=cpb)
+        sh = stream.cuda_stream
+        w.step(1, sh)  # graph capture
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        w.step(steps - 1, sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st, ov = w.stats()
+        hs = w.host_scene(0)
+        w.close()
+        t_gpu, g = _solve_timed(lib, cfg, hs, dt)
+        mcfg = abi.default_config(**{n: getattr(cfg, n) for n, _ in abi.Config._fields_})
+        mcfg.precision = abi.PDC_PRECISION_MIXED
+        t_mix, m = _solve_timed(lib, mcfg, hs, dt)
+        entry = {"workload": desc, "steps_timed": steps - 1, "ms_per_step": ms / (steps - 1),
+                 "value": (steps - 1) / (ms / 1e3), "unit": "steps/s", "bodies": int(len(sc["type"])),
+                 "contacts_last_step": int(hs.n_contacts), "dropped_contact_points": int(ov.sum()),
+                 "last_step": {k: st[0][k] for k in ("status", "newton_iters", "pcg_iters", "team", "exit_err")},
+                 "final_contact_set": {
+                     "fp64_ms": t_gpu * 1e3, "mixed_ms": t_mix * 1e3,
+                     "fp64": {k: g[3][k] for k in ("status", "newton_iters", "pcg_iters", "n_local_bodies",
+                                                    "kkt_stationarity", "kkt_complementarity", "kkt_cone")},
+                     "mixed": {k: m[3][k] for k in ("status", "newton_iters", "pcg_iters",
+                                                     "kkt_stationarity", "kkt_complementarity", "kkt_cone")}}}
+        if cpu_cores:
+            import oracle_lib  # the reference algorithm's CPU implementation (checker only)
+
+            t0 = time.perf_counter()
+            o = oracle_lib.solve(hs, dt=dt, cfg=cfg, nthreads=cpu_cores)
+            t_cpu = time.perf_counter() - t0
+            ov_ = np.concatenate([o[0], o[1]], 1)
+            scale = max(float(np.abs(ov_).max()), 9.81 * dt)
+            err = lambda r: float(np.abs(np.concatenate([r[0], r[1]], 1) - ov_).max() / scale)
+            fc = entry["final_contact_set"]
+            fc["cpu_oracle_ms"] = t_cpu * 1e3
+            fc["cpu_cores"] = cpu_cores
+            fc["cpu_oracle"] = {k: o[3][k] for k in ("status", "newton_iters", "pcg_iters")}
+            fc["fp64_velocity_err_vs_oracle"] = err(g)
+            fc["mixed_velocity_err_vs_oracle"] = err(m)
+        out[name] = entry
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,6 +312,9 @@ def main():
     ap.add_argument("--single-sample", type=int, default=256)
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--pit-steps", type=int, default=200)
+    ap.add_argument("--pile-steps", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = abi.default_config(tol=args.tol, sparse_max_bodies=args.sparse_max,
@@ -369,11 +456,15 @@ def main():
     if not args.no_world:
         line["world"] = run_world(args, cfg, lib, torch, stream, local, rank, world)
 
+    cores = 0
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib
 
         cores = oracle_lib.load().pdc_oracle_physical_processors()
+    if not args.no_large and world == 1:  # single scenes: not sharded (replicas only)
+        line["large"] = run_large(args, cfg, lib, torch, stream, cores)
+    if cores:
         tc = cpu_reference(batch, cfg, args.cpu_sample, cores)
         line["cpu_baseline"] = {"value": args.cpu_sample / tc, "unit": METRIC, "cores": cores, "kind": "port",
                                 "sample": f"first {args.cpu_sample} of {args.scenes} scenes, one pass, "

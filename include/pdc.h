@@ -84,6 +84,13 @@ typedef struct pdc_config {
     int32_t force_model;      /* enum pdc_force_model */
     int32_t spring_based;     /* non_smooth_force.spring_based_force (0) */
     double mu;                /* non_smooth_force.static_coeff (0.5) */
+    double mu_pair_lo;        /* per-pair friction (no counterpart in the reference, whose mu
+                                 is global): when mu_pair_hi > mu_pair_lo, contacts without
+                                 an explicit mu between scene-local bodies i, j get
+                                 mu = fma(hi - lo, u, lo), u = (splitmix64(seed ^ key) >> 11)
+                                 * 2^-53, key = (min(i,j) << 32) | max(i,j) (0, 0: off) */
+    double mu_pair_hi;
+    uint64_t mu_pair_seed;
     double restitution;       /* non_smooth_force.restitution (0.0; only_normal: 0.5) */
     double spring_k;          /* non_smooth_force.spring_k (1e6) */
     double spring_damp;       /* non_smooth_force.spring_damp (0.01) */

@@ -32,7 +32,9 @@
 // (SA-AMG + Gauss-Seidel + CG, tol 1e-8, maxiter 1000), which is absent: this
 // oracle substitutes a block-Jacobi CG with the same tolerance, iteration cap,
 // initial guess and Hu rule (:395-427, :474-479).
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -86,6 +88,18 @@ int physical_processors() {
 // LorentzCircleConstraint.cpp:5-55, m_perturbation = 1e-16, m_shift = 1e-8 (.h:18-19).
 static const Real kPert = 1e-16;
 static const Real kShift = 1e-8;
+// Per-pair friction (pdc_config.mu_pair_*; the reference's mu is global): the
+// splitmix64 finaliser (Steele, Lea, Flood 2014) of seed ^ ((min << 32) | max),
+// its top 53 bits as u in [0, 1), mu = fma(hi - lo, u, lo).
+static inline double pair_mu(int i, int j, const pdc_config& c) {
+    const uint64_t a = (uint32_t)std::min(i, j), b = (uint32_t)std::max(i, j);
+    uint64_t z = (c.mu_pair_seed ^ ((a << 32) | b)) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return std::fma(c.mu_pair_hi - c.mu_pair_lo, (double)(z >> 11) * 0x1.0p-53, c.mu_pair_lo);
+}
+
 static inline Real cone_c(const Real* f, Real mu) {
     Real r = f[1] * f[1] + f[2] * f[2] + kPert;
     return std::sqrt(r) - mu * f[0] - std::sqrt(kPert) - kShift;
@@ -1093,7 +1107,10 @@ extern "C" int pdc_oracle_solve(const pdc_config* cfg, double dt, const double g
                 }
             }
         }
-        P.mu[c] = contacts->mu ? contacts->mu[c] : cfg->mu;
+        if (contacts->mu) P.mu[c] = contacts->mu[c];
+        else if (cfg->mu_pair_hi > cfg->mu_pair_lo)
+            P.mu[c] = pair_mu(contacts->body[2 * c], contacts->body[2 * c + 1], *cfg);
+        else P.mu[c] = cfg->mu;
         P.depth[c] = contacts->depth ? contacts->depth[c] : 0.0;
     }
     fill_forces_intl(P, &out->stats);

@@ -37,6 +37,9 @@ class Config(C.Structure):
         ("force_model", C.c_int32),
         ("spring_based", C.c_int32),
         ("mu", C.c_double),
+        ("mu_pair_lo", C.c_double),
+        ("mu_pair_hi", C.c_double),
+        ("mu_pair_seed", C.c_uint64),
         ("restitution", C.c_double),
         ("spring_k", C.c_double),
         ("spring_damp", C.c_double),
@@ -192,6 +195,9 @@ def default_config(**overrides):
     cfg.force_model = PDC_FORCE_NON_SMOOTH_CONTACT
     cfg.spring_based = 0
     cfg.mu = 0.5
+    cfg.mu_pair_lo = 0.0
+    cfg.mu_pair_hi = 0.0
+    cfg.mu_pair_seed = 0
     cfg.restitution = 0.0
     cfg.spring_k = 1e6
     cfg.spring_damp = 0.01

@@ -84,6 +84,9 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.max_iter = c.max_iter;
     e.tol = c.tol;
     e.mu = c.mu;
+    e.mu_pair_lo = c.mu_pair_lo;
+    e.mu_pair_hi = c.mu_pair_hi;
+    e.mu_pair_seed = c.mu_pair_seed;
     e.restitution = c.restitution;
     e.spring_based = c.spring_based;
     e.compliance_coef = 0;
@@ -225,6 +228,9 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->force_model = PDC_FORCE_NON_SMOOTH_CONTACT;
     c->spring_based = 0;
     c->mu = 0.5;         // NonSmoothContactForce.cpp:332
+    c->mu_pair_lo = 0.0;
+    c->mu_pair_hi = 0.0;
+    c->mu_pair_seed = 0;
     c->restitution = 0;  // :329
     c->spring_k = 1e6;   // :324
     c->spring_damp = 0.01;
@@ -255,6 +261,7 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
     if (c->precision != PDC_PRECISION_FP64 && c->precision != PDC_PRECISION_MIXED)
         return fail(s, PDC_EINVAL, "unknown precision");
     if (c->pcg_max_direct <= 0 || c->pcg_max_iter <= 0) return fail(s, PDC_EINVAL, "bad PCG caps");
+    if (c->mu_pair_hi > c->mu_pair_lo && !(c->mu_pair_lo >= 0)) return fail(s, PDC_EINVAL, "negative mu_pair_lo");
     if (c->pcg_lanes != 0 && c->pcg_lanes != 1 && c->pcg_lanes != 2 && c->pcg_lanes != 4 && c->pcg_lanes != 8)
         return fail(s, PDC_EINVAL, "pcg_lanes not in {0, 1, 2, 4, 8}");
     if (c->sparse_max_bodies < 0 || c->sparse_max_bodies > pdc::kSparseMax)

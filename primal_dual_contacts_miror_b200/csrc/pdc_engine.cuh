@@ -28,6 +28,8 @@ struct EngineCfg {
     int max_iter;
     double tol;
     double mu;
+    double mu_pair_lo, mu_pair_hi;  // per-pair friction when hi > lo
+    unsigned long long mu_pair_seed;
     double restitution;
     int spring_based;
     double compliance_coef;  // m_compliance numerator inputs
@@ -165,6 +167,18 @@ __device__ __forceinline__ d3 sym_mul(const double* W, d3 v) {
               W[4] * v.x + W[5] * v.y + W[2] * v.z};
 }
 
+// Per-pair friction coefficient of scene-local bodies i, j: splitmix64 of the
+// seed xor the ordered pair key, top 53 bits as u in [0, 1), mu = lo + (hi-lo) u.
+__device__ __forceinline__ double pair_mu(int i, int j, double lo, double hi, unsigned long long seed) {
+    const unsigned long long a = (unsigned long long)(unsigned)min(i, j), b = (unsigned long long)(unsigned)max(i, j);
+    unsigned long long z = (seed ^ ((a << 32) | b)) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * 0x1.0p-53;
+    return fma(hi - lo, u, lo);
+}
+
 // Velocity of the contact point on body j: v + w x c  (zero for static / non-active)
 __device__ __forceinline__ d3 point_vel(const double* u6, d3 c) {
     d3 v = ld3(u6), w = ld3(u6 + 3);
@@ -219,7 +233,12 @@ class SceneSolver {
         return t;
     }
     __device__ __forceinline__ bool active(int gb) const { return B.local[gb] && !B.is_static[gb]; }
-    __device__ __forceinline__ double cmu(int gc) const { return B.cmu ? B.cmu[gc] : C.mu; }
+    __device__ __forceinline__ double cmu(int gc) const {
+        if (B.cmu) return B.cmu[gc];
+        if (C.mu_pair_hi > C.mu_pair_lo)
+            return pair_mu(B.cbody[2 * gc], B.cbody[2 * gc + 1], C.mu_pair_lo, C.mu_pair_hi, C.mu_pair_seed);
+        return C.mu;
+    }
 
     // Gather sum over the incidences of body gb of sigma * [X; c x X]
     __device__ __forceinline__ void gather(int gb, double out[6]) const {

@@ -190,6 +190,32 @@ class World:
         return counts, {"body": body[:n], "frame": frame[:n], "arm": arm[:n], "depth": depth[:n], "pos": pos[:n],
                         "local_force": lf[:n]}
 
+    def host_scene(self, k=0):
+        """Scene k as the contact problem its next step would solve: contacts
+        regenerated from the current poses (collide), body state with world-frame
+        inertia, scene-local body ids -- a HostScene for Solver.solve or any
+        other solver of the same interface."""
+        self.collide()
+        self.sync()
+        pos, quat, vel, ang = self.state()
+        counts, c = self.contacts()
+        b0, b1 = int(self.shapes.body_offsets[k]), int(self.shapes.body_offsets[k + 1])
+        c0 = int(counts[:k].sum())
+        c1 = c0 + int(counts[k])
+        q = quat[b0:b1]
+        x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+        R = np.stack([
+            np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+            np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+            np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+        i0 = self.shapes.inertia0[b0:b1]
+        iw = np.einsum("nij,nj,nkj->nik", R, i0, R)
+        iwi = np.einsum("nij,nj,nkj->nik", R, 1.0 / i0, R)
+        s6 = lambda m: np.stack([m[:, 0, 0], m[:, 1, 1], m[:, 2, 2], m[:, 0, 1], m[:, 0, 2], m[:, 1, 2]], -1)
+        return abi.HostScene(vel[b0:b1], ang[b0:b1], self.shapes.mass[b0:b1], s6(iw), s6(iwi),
+                             self.shapes.is_static[b0:b1], c["body"][c0:c1], c["frame"][c0:c1], c["arm"][c0:c1],
+                             c["depth"][c0:c1])
+
     def stats(self):
         ns = self.shapes.n_scenes
         st = (abi.Stats * ns)()

@@ -85,6 +85,21 @@ def test_stack_resultants_match(gpu):
     assert rel(np.concatenate([dv, da], 1), np.concatenate([odv, oda], 1), 0.0981) < 1e-7
 
 
+@pytest.mark.parametrize("seed", [1, 2024])
+def test_pair_mu_matches_oracle(gpu, seed):
+    """Per-pair friction (mu ~ U[0.3, 0.8] hashed from the body pair) on a
+    multi-column scene and a batch of piles: GPU against the oracle at 1e-9."""
+    cfg = abi.default_config(tol=1e-8, mu_pair_lo=0.3, mu_pair_hi=0.8, mu_pair_seed=seed)
+    s = scenes.box_columns(9, 4, seed=5, vel_noise=0.01, tilt=0.0)
+    compare(gpu.Solver(cfg).solve(s), oracle_lib.solve(s, cfg=cfg))
+    sc = scenes.pile_batch(16, seed=seed, n_min=4, n_max=64)
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    dv, da, lf, st = gpu.Solver(cfg).batch_solve(batch)
+    odv, oda, olf, ost = oracle_lib.batch_solve(batch, cfg=cfg)
+    assert rel(lf, olf) < 1e-9
+    assert rel(np.concatenate([dv, da], 1), np.concatenate([odv, oda], 1), 0.0981) < 1e-9
+
+
 def test_known_answers_on_gpu(gpu):
     s = scenes.resting_box_stack(10)
     solver = gpu.Solver(abi.default_config(tol=1e-8))

@@ -49,6 +49,31 @@ def test_sliding_sphere_decelerates_by_mu_g_dt():
     assert da[1, 1] == pytest.approx(2.5 * 0.5 * G * DT / 0.5, rel=1e-6)
 
 
+def pair_mu_py(i, j, lo, hi, seed):
+    """Independent Python statement of the per-pair friction of pdc_config:
+    splitmix64(seed ^ ((min << 32) | max)), top 53 bits as u, mu = lo + (hi-lo) u."""
+    M = (1 << 64) - 1
+    z = (seed ^ ((min(i, j) << 32) | max(i, j))) + 0x9E3779B97F4A7C15 & M
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+    z ^= z >> 31
+    return lo + (hi - lo) * ((z >> 11) * 2.0 ** -53)
+
+
+@pytest.mark.parametrize("seed", [0, 7, 2 ** 63 + 12345])
+def test_sliding_sphere_uses_pair_mu(seed):
+    """Per-pair friction (beyond the reference's global mu): the sliding sphere
+    (bodies 0 = ground, 1 = sphere) decelerates by mu_pair(0, 1) g dt."""
+    mu = pair_mu_py(0, 1, 0.3, 0.8, seed)
+    assert 0.3 <= mu < 0.8
+    s = scenes.sliding_sphere(vel=(3.0, 0, 0))
+    cfg = abi.default_config(tol=1e-10, mu_pair_lo=0.3, mu_pair_hi=0.8, mu_pair_seed=seed)
+    dv, da, lf, st = oracle_lib.solve(s, cfg=cfg)
+    # the smoothed cone (perturbation and shift terms) leaves ~3e-7 in the effective mu
+    assert dv[1, 0] == pytest.approx(-mu * G * DT, rel=2e-6)
+    assert lf[0, 1] ** 2 + lf[0, 2] ** 2 == pytest.approx((mu * lf[0, 0]) ** 2, rel=1e-5)
+
+
 def test_stack_levels_carry_weight_above():
     s = scenes.resting_box_stack(10)
     dv, da, lf, st = oracle_lib.solve(s, cfg=abi.default_config(tol=1e-8))
