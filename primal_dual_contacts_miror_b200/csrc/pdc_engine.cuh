@@ -169,7 +169,7 @@ __device__ __forceinline__ d3 sym_mul(const double* W, d3 v) {
 
 // Per-pair friction coefficient of scene-local bodies i, j: splitmix64 of the
 // seed xor the ordered pair key, top 53 bits as u in [0, 1), mu = lo + (hi-lo) u.
-__device__ __forceinline__ double pair_mu(int i, int j, double lo, double hi, unsigned long long seed) {
+__device__ __noinline__ double pair_mu(int i, int j, double lo, double hi, unsigned long long seed) {
     const unsigned long long a = (unsigned long long)(unsigned)min(i, j), b = (unsigned long long)(unsigned)max(i, j);
     unsigned long long z = (seed ^ ((a << 32) | b)) + 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -698,7 +698,8 @@ class SceneSolver {
 
             // ---- linear solve: block-Jacobi PCG (replaces LDLT / AMGCL, :385-427)
             const double rtol = direct ? C.rtol_direct : C.rtol_iter;
-            const int lanes = (C.pcg_lanes > 0 && nt % 32 == 0) ? C.pcg_lanes : Team::spmv_lanes;
+            // lanes per body in the PCG product: chosen for the large-scene teams only
+            const int lanes = (Team::spmv_lanes > 1 && C.pcg_lanes > 0) ? C.pcg_lanes : Team::spmv_lanes;
             const int maxit = direct ? C.max_direct : C.max_cg;
             int iters = 0;
             bool lin_bad = false;
@@ -749,11 +750,28 @@ class SceneSolver {
                     const double* pp = (iters & 1) ? B.p2 : B.p;
                     double* pc = (iters & 1) ? B.p : B.p2;
                     double s3[1] = {0};
-                    switch (lanes) {
-                        case 8: pcg_product<8>(pp, pc, beta, eps, s3[0]); break;
-                        case 4: pcg_product<4>(pp, pc, beta, eps, s3[0]); break;
-                        case 2: pcg_product<2>(pp, pc, beta, eps, s3[0]); break;
-                        default: pcg_product<1>(pp, pc, beta, eps, s3[0]); break;
+                    if constexpr (Team::spmv_lanes > 1) {
+                        switch (lanes) {
+                            case 8: pcg_product<8>(pp, pc, beta, eps, s3[0]); break;
+                            case 4: pcg_product<4>(pp, pc, beta, eps, s3[0]); break;
+                            case 2: pcg_product<2>(pp, pc, beta, eps, s3[0]); break;
+                            default: pcg_product<1>(pp, pc, beta, eps, s3[0]); break;
+                        }
+                    } else {
+                        for (int i = tid; i < n_local; i += nt) {
+                            const int gb = B.lbody[b0 + i];
+                            if (!active(gb)) continue;
+                            double pn[6], q6[6];
+                            for (int r = 0; r < 6; ++r) {
+                                pn[r] = __dadd_rn(B.z[6 * gb + r], __dmul_rn(beta, pp[6 * gb + r]));
+                                pc[6 * gb + r] = pn[r];
+                            }
+                            spmv_body_fused1(gb, pn, pp, beta, eps, q6);
+                            for (int r = 0; r < 6; ++r) {
+                                s3[0] += pn[r] * q6[r];
+                                B.q[6 * gb + r] = q6[r];
+                            }
+                        }
                     }
                     T.sum(s3);
                     const double alpha = rz / s3[0];
@@ -1487,6 +1505,39 @@ class SceneSolver {
     // contact's X = W (v1p - v0p) recomputed here (the other body's direction
     // from z + beta pp) instead of read from a contact phase: the same operations
     // as spmv_to_X + spmv_body, so the same bits, with no barrier between them.
+    // One lane per body (block and warp teams): the same sums as the L = 1 case
+    // of spmv_body_fused below, kept as its own loop for the block kernel's code.
+    __device__ __forceinline__ void spmv_body_fused1(int gb, const double* pn, const double* pp, double beta,
+                                                     double eps, double* q6) const {
+        double y[6];
+        mass_mul(gb, pn, y);
+        const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+#pragma unroll 2
+        for (int k = 0; k < n; ++k) {
+            const int e = B.inc[st + k], go = B.inc_o[st + k];
+            const int gc = e >> 1, side = e & 1;
+            const d3 arm = ld3(B.arm + 6 * gc + 3 * side);
+            const d3 pv_own = point_vel(pn, arm);
+            d3 pv_oth = d3{0, 0, 0};
+            if (go >= 0) {
+                double po[6];
+                for (int r = 0; r < 6; ++r) po[r] = __dadd_rn(B.z[6 * go + r], __dmul_rn(beta, pp[6 * go + r]));
+                pv_oth = point_vel(po, ld3(B.arm + 6 * gc + 3 * (1 - side)));
+            }
+            d3 x = sym_mul(B.W + 6 * gc, side ? sub3(pv_own, pv_oth) : sub3(pv_oth, pv_own));
+            if (!side) x = scl3(-1.0, x);
+            const d3 t = cross3(arm, x);
+            a0 += x.x; a1 += x.y; a2 += x.z;
+            a3 += t.x; a4 += t.y; a5 += t.z;
+        }
+        q6[0] = y[0] + eps * pn[0] + a0;
+        q6[1] = y[1] + eps * pn[1] + a1;
+        q6[2] = y[2] + eps * pn[2] + a2;
+        q6[3] = y[3] + eps * pn[3] + a3;
+        q6[4] = y[4] + eps * pn[4] + a4;
+        q6[5] = y[5] + eps * pn[5] + a5;
+    }
     // PCG product of every active body: p_new = z + beta pp into pc, q = A p_new,
     // and this thread's share of p_new . q.  L lanes per body split its
     // incidences; the loop runs in rounds so every lane of a warp takes the same

@@ -42,19 +42,21 @@ def test_large_teams_match_block_team(team):
         assert abs(big[3][k]["newton_iters"] - blk[3][k]["newton_iters"]) <= 1
 
 
-@pytest.mark.parametrize("lanes", [2, 4, 8])
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8])
 def test_pcg_lanes_agree(lanes):
-    """The PCG product with several lanes per body (incidences split across
-    lanes, partials combined by shuffles) against one lane per body, on a block
-    team and on the whole GPU: the same solve up to round-off."""
+    """The large-scene teams' PCG product with several lanes per body
+    (incidences split across lanes, partials combined by shuffles), on the whole
+    GPU and on a cluster, against the block team's one lane per body: the same
+    solve up to round-off."""
     from primal_dual_contacts_miror_b200 import lib
 
     s = scenes.settled_pile(400, np.random.default_rng(5), vel_noise=0.01)
-    for gmin in (0, 8):
-        one = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=gmin, pcg_lanes=1)).solve(s)
-        many = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=gmin, pcg_lanes=lanes,
-                                             cluster_max_contacts=-1)).solve(s)
-        assert one[3]["pcg_iters"] > 0
+    one = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=0)).solve(s)
+    assert one[3]["pcg_iters"] > 0 and one[3]["team"] == 0
+    for kind, cmax in TEAMS.values():
+        many = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8, pcg_lanes=lanes,
+                                             cluster_max_contacts=cmax)).solve(s)
+        assert many[3]["team"] == kind
         assert _rel(many[2], one[2]) < 1e-9
         v1 = np.concatenate([one[0], one[1]], 1)
         vm = np.concatenate([many[0], many[1]], 1)
