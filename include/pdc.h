@@ -106,9 +106,11 @@ typedef struct pdc_config {
     int32_t grid_min_bodies;   /* scenes with at least this many bodies are large: solved one
                                   launch each, by a thread-block cluster or the whole GPU
                                   (1024; 0 = never) */
-    int32_t cluster_max_contacts; /* a large scene with at most this many contacts is solved by
-                                  one thread-block cluster (up to 16 CTAs), above it by the
-                                  whole GPU (cooperative launch) (4096; -1 = never) */
+    int32_t cluster_max_contacts; /* a large scene with at most this many contacts and at most
+                                  cluster_max_bodies bodies is solved by one thread-block
+                                  cluster (up to 16 CTAs), else by the whole GPU (cooperative
+                                  launch) (4096; -1 = never) */
+    int32_t cluster_max_bodies; /* (4096) */
     int32_t pcg_lanes;         /* lanes per body in the PCG product: 1, 2, 4 or 8 (0 = 1 for
                                   block and warp teams, 4 for the large-scene teams) */
     double pcg_rtol_direct;   /* PCG relative residual standing in for LDLT (1e-13) */

@@ -51,6 +51,7 @@ class Config(C.Structure):
         ("cta_threads", C.c_int32),
         ("grid_min_bodies", C.c_int32),
         ("cluster_max_contacts", C.c_int32),
+        ("cluster_max_bodies", C.c_int32),
         ("pcg_lanes", C.c_int32),
         ("pcg_rtol_direct", C.c_double),
         ("pcg_max_direct", C.c_int32),
@@ -209,6 +210,7 @@ def default_config(**overrides):
     cfg.cta_threads = 256
     cfg.grid_min_bodies = 1024
     cfg.cluster_max_contacts = 4096
+    cfg.cluster_max_bodies = 4096
     cfg.pcg_lanes = 0
     cfg.pcg_rtol_direct = 1e-13
     cfg.pcg_max_direct = 4000

@@ -98,6 +98,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.warp_max_bodies = c.warp_max_bodies;
     e.grid_min_bodies = c.grid_min_bodies;
     e.cluster_max_contacts = c.cluster_max_contacts;
+    e.cluster_max_bodies = c.cluster_max_bodies;
     e.pcg_lanes = c.pcg_lanes;
     e.mixed = c.precision == PDC_PRECISION_MIXED;
     e.inner_rtol = c.mixed_inner_rtol;
@@ -242,6 +243,7 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->cta_threads = 256;
     c->grid_min_bodies = 1024;
     c->cluster_max_contacts = 4096;
+    c->cluster_max_bodies = 4096;
     c->pcg_lanes = 0;
     c->pcg_rtol_direct = 1e-13;
     c->pcg_max_direct = 4000;

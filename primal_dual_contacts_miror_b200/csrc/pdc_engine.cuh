@@ -40,6 +40,7 @@ struct EngineCfg {
     int warp_max_bodies;
     int grid_min_bodies;   // scenes with at least this many bodies are large
     int cluster_max_contacts;  // large scenes up to this many contacts go to a cluster team
+    int cluster_max_bodies;    // ... if they have at most this many bodies
     int pcg_lanes;             // lanes per body in the PCG product (0: the team's default)
     int mixed;             // FP32 inner PCG + FP64 iterative refinement
     double inner_rtol;     // FP32 inner solve relative residual
@@ -1930,11 +1931,18 @@ __global__ void __launch_bounds__(THREADS) solve_scenes_kernel(const __grid_cons
 
 // Team of a large scene, decided on the device from its current contact count
 // (the world's counts are only known there): a cluster team up to
-// C.cluster_max_contacts contacts, the whole GPU above.
+// C.cluster_max_contacts contacts and C.cluster_max_bodies bodies, else the
+// whole GPU.
 __device__ __forceinline__ bool large_on_cluster(const BatchPtrs& B, const EngineCfg& C, int s) {
-    const int nc = B.body_off ? (B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - B.contact_off[s])
-                              : B.single_nc;
-    return nc <= C.cluster_max_contacts;
+    int nb, nc;
+    if (B.body_off) {
+        nb = B.body_cnt ? B.body_cnt[s] : B.body_off[s + 1] - B.body_off[s];
+        nc = B.contact_cnt ? B.contact_cnt[s] : B.contact_off[s + 1] - B.contact_off[s];
+    } else {
+        nb = B.single_nb;
+        nc = B.single_nc;
+    }
+    return nc <= C.cluster_max_contacts && nb <= C.cluster_max_bodies;
 }
 
 // One large scene solved by the whole GPU (cooperative launch, grid team).

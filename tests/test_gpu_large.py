@@ -16,6 +16,7 @@ def _rel(a, b, floor=0.0):
 
 # team kinds in pdc_stats.team, and the cluster_max_contacts that routes a large scene to them
 TEAMS = {"grid": (2, -1), "cluster": (3, 1 << 30)}
+BIG = 1 << 30
 
 
 @pytest.mark.parametrize("team", sorted(TEAMS))
@@ -30,7 +31,8 @@ def test_large_teams_match_block_team(team):
     sc.append(scenes.settled_pile(300, np.random.default_rng(3), vel_noise=0.01))  # PCG (> 256 bodies)
     batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
     blk = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=0)).batch_solve(batch)
-    big = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8, cluster_max_contacts=cmax)).batch_solve(batch)
+    big = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8, cluster_max_contacts=cmax,
+                                        cluster_max_bodies=BIG)).batch_solve(batch)
     for k in range(len(sc)):
         b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
         c0, c1 = batch.contact_offsets[k], batch.contact_offsets[k + 1]
@@ -55,7 +57,7 @@ def test_pcg_lanes_agree(lanes):
     assert one[3]["pcg_iters"] > 0 and one[3]["team"] == 0
     for kind, cmax in TEAMS.values():
         many = lib.Solver(abi.default_config(tol=1e-8, grid_min_bodies=8, pcg_lanes=lanes,
-                                             cluster_max_contacts=cmax)).solve(s)
+                                             cluster_max_contacts=cmax, cluster_max_bodies=BIG)).solve(s)
         assert many[3]["team"] == kind
         assert _rel(many[2], one[2]) < 1e-9
         v1 = np.concatenate([one[0], one[1]], 1)
@@ -80,7 +82,8 @@ def test_large_pile_matches_oracle(n_boxes, tol, bar, team):
     kind, cmax = TEAMS[team]
     s = scenes.settled_pile(n_boxes, np.random.default_rng(n_boxes), vel_noise=0.01)
     cfg = abi.default_config(tol=tol)
-    dv, da, lf, st = lib.Solver(abi.default_config(tol=tol, cluster_max_contacts=cmax)).solve(s)
+    dv, da, lf, st = lib.Solver(abi.default_config(tol=tol, cluster_max_contacts=cmax,
+                                                   cluster_max_bodies=BIG)).solve(s)
     if n_boxes not in _ORACLE:
         _ORACLE[n_boxes] = oracle_lib.solve(s, cfg=cfg, nthreads=8)
     odv, oda, olf, ost = _ORACLE[n_boxes]
