@@ -34,6 +34,8 @@ from primal_dual_contacts_miror_b200 import abi, scenes  # noqa: E402
 
 METRIC = "scene-steps/s"
 SEED = 20241203 + 3 * 10 ** 6
+# DRAM bytes of one solve_scenes_kernel launch on the 4,096-scene workload (ncu capture)
+TRAFFIC_PER_LAUNCH = 15.21e9
 
 
 def algorithmic_bytes(stats, n_contacts):
@@ -294,6 +296,29 @@ def run_large(args, base_cfg, lib, torch, stream, cpu_cores):
     return out
 
 
+def run_serving(args, base_cfg, lib, torch):
+    """Continuous batching under Poisson arrivals: requests are box drops of
+    n ~ log-uniform[8, 512] boxes with horizons U{50..500} steps (mu 0.5,
+    dt 0.01), admitted into a server whose body pool is sized from a 150 GB
+    device budget (capped at slots x 512 bodies).  One fresh server per rate;
+    per-tick (one step of every admitted scene) device time gives p50/p99."""
+    from primal_dual_contacts_miror_b200 import serving
+
+    budget = 150e9
+    slots = args.serve_slots
+    pool = min(serving.capacity_for_budget(budget), slots * 512)
+    out = {"budget_bytes": budget, "slots": slots, "pool_bodies": pool, "ticks_per_rate": args.serve_ticks,
+           "workload": "Poisson box-drop requests, 8-512 boxes log-uniform, horizon U{50..500}, dt 0.01",
+           "rates": []}
+    cfg = abi.default_config(**{n: getattr(base_cfg, n) for n, _ in abi.Config._fields_})
+    for rate in [float(r) for r in args.serve_rates.split(",") if r]:
+        srv = lib.Server(slots, pool, dt=0.01, cfg=cfg)
+        res = serving.run(srv, rate, args.serve_ticks, seed=20241203 + 4 * 10 ** 6 + int(rate), torch=torch)
+        srv.close()
+        out["rates"].append(res)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -315,6 +340,10 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--pit-steps", type=int, default=200)
     ap.add_argument("--pile-steps", type=int, default=200)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rates", default="1000,5000,20000,50000")
+    ap.add_argument("--serve-slots", type=int, default=2048)
+    ap.add_argument("--serve-ticks", type=int, default=40)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = abi.default_config(tol=args.tol, sparse_max_bodies=args.sparse_max,
@@ -409,7 +438,9 @@ def main():
         "gpu_launches": 2 * args.steps,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if args.scenes == 4096 else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this "
+                                       "kernel on this workload", "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": ab, "kernel": "solve_scenes_kernel"},
         "clocks": clk,
     }
@@ -464,6 +495,8 @@ def main():
         cores = oracle_lib.load().pdc_oracle_physical_processors()
     if not args.no_large and world == 1:  # single scenes: not sharded (replicas only)
         line["large"] = run_large(args, cfg, lib, torch, stream, cores)
+    if not args.no_serve and world == 1:
+        line["serving"] = run_serving(args, cfg, lib, torch)
     if cores:
         tc = cpu_reference(batch, cfg, args.cpu_sample, cores)
         line["cpu_baseline"] = {"value": args.cpu_sample / tc, "unit": METRIC, "cores": cores, "kind": "port",

@@ -34,7 +34,7 @@ def run(server, rate, n_ticks, seed, n_min=8, n_max=512, h_min=50, h_max=500, wa
     sh = stream.cuda_stream if stream is not None else 0
     clock = 0.0
     next_arrival = rng.exponential(1.0 / rate)
-    queue = []  # (arrival_time, scene, horizon)
+    queue = []  # [arrival_time, boxes, horizon, scene seed, scene (built when it reaches the head)]
     admitted_at = {}
     tick_ms = []
     waits = []
@@ -45,10 +45,13 @@ def run(server, rate, n_ticks, seed, n_min=8, n_max=512, h_min=50, h_max=500, wa
     for t in range(n_ticks + warmup_ticks):
         while next_arrival <= clock:
             n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
-            queue.append((next_arrival, scenes.box_drop_world(n, rng), int(rng.integers(h_min, h_max + 1))))
+            queue.append([next_arrival, n, int(rng.integers(h_min, h_max + 1)), int(rng.integers(1 << 62)), None])
             next_arrival += rng.exponential(1.0 / rate)
         while queue:
-            arr, sc, hz = queue[0]
+            head = queue[0]
+            if head[4] is None:  # requests are built when they can first be admitted
+                head[4] = scenes.box_drop_world(head[1], np.random.default_rng(head[3]))
+            arr, hz, sc = head[0], head[2], head[4]
             slot = server.admit(sc, hz)
             if slot is None:
                 break
