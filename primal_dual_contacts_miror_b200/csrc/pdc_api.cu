@@ -89,6 +89,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.mu_pair_seed = c.mu_pair_seed;
     e.restitution = c.restitution;
     e.spring_based = c.spring_based;
+    e.only_normal = c.force_model == PDC_FORCE_ONLY_NORMAL;
     e.compliance_coef = 0;
     e.spring_k = c.spring_k;
     e.spring_damp = c.spring_damp;
@@ -258,8 +259,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
     if (!c) return fail(s, PDC_EINVAL, "null config");
     if (c->abi_version != PDC_ABI_VERSION) return fail(s, PDC_EINVAL, "ABI version mismatch");
     if (c->max_iter < 0 || !(c->tol >= 0)) return fail(s, PDC_EINVAL, "bad iterations/tolerance");
-    if (c->force_model != PDC_FORCE_NON_SMOOTH_CONTACT)
-        return fail(s, PDC_EINVAL, "non-smooth force model not supported by the GPU path");
+    if (c->force_model != PDC_FORCE_NON_SMOOTH_CONTACT && c->force_model != PDC_FORCE_ONLY_NORMAL)
+        return fail(s, PDC_EINVAL, "unknown non-smooth force model");
     if (c->precision != PDC_PRECISION_FP64 && c->precision != PDC_PRECISION_MIXED)
         return fail(s, PDC_EINVAL, "unknown precision");
     if (c->pcg_max_direct <= 0 || c->pcg_max_iter <= 0) return fail(s, PDC_EINVAL, "bad PCG caps");

@@ -32,6 +32,7 @@ struct EngineCfg {
     unsigned long long mu_pair_seed;
     double restitution;
     int spring_based;
+    int only_normal;   // OnlyNormalForce (OnlyNormalForce.cpp:7-217): 1-D force, no friction
     double compliance_coef;  // m_compliance numerator inputs
     double spring_k, spring_damp;
     int direct_threshold;
@@ -442,7 +443,7 @@ class SceneSolver {
             B.f[3 * gc + 1] = 0;
             B.f[3 * gc + 2] = 0;
             B.lam[2 * gc] = 1e-2;
-            B.lam[2 * gc + 1] = 1e-2;
+            B.lam[2 * gc + 1] = C.only_normal ? 0.0 : 1e-2;  // only_normal: lambda_t absent
         }
         T.sync();
         return true;
@@ -482,6 +483,27 @@ class SceneSolver {
         return dmin(rad / (tn + 1e-8) * fw, 1.0);
     }
 
+    // OnlyNormalForce residuals (OnlyNormalForce.cpp:46-89) and AC term (:202-217):
+    // rf = -w_n (- compliance f_n) + lambda - k, rl = lambda (-f_n) + mu_c, unit
+    // weight, AC = max(f_n - (w_n + k + spring f_n), 0) - f_n; X = -R (f_n, 0, 0).
+    __device__ __forceinline__ void normal_residual(int gc, const Frame& R, d3 w, double fn, double ln, double muc,
+                                                    double* rfo, double* rlo, double& wrf2, double& rl2,
+                                                    double& ac2) const {
+        double r0 = 0 - w.x;
+        if (C.spring_based) r0 -= compliance * cm * fn;
+        r0 += ln;
+        r0 -= B.kn[gc];
+        const double rl0 = ln * (-fn) + muc;
+        wrf2 += r0 * r0;
+        rl2 += rl0 * rl0;
+        const double tp = fn - (w.x + B.kn[gc] + spring_term * fn);
+        const double a0 = dmax(tp, 0.0) - fn;
+        ac2 += a0 * a0;
+        if (rfo) { rfo[0] = r0; rfo[1] = 0; rfo[2] = 0; }
+        if (rlo) { rlo[0] = rl0; rlo[1] = 0; }
+        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, 0.0, 0.0})));
+    }
+
     // Residual terms of one contact at state (uvec, f, lam) (nonSmoothResiduals :119-172,
     // ACVector :53-73).  Writes X = -R f for the ru gather; returns squared norms.
     __device__ __forceinline__ void contact_residual(int gc, const double* uvec, const double* fv, const double* lv,
@@ -489,6 +511,10 @@ class SceneSolver {
                                                      double& wrf2, double& rl2, double& ac2) const {
         const Frame R = ld_frame(B.frame + 9 * gc);
         const d3 w = rel_vel(gc, uvec);
+        if (C.only_normal) {
+            normal_residual(gc, R, w, fv[0], lv[0], muc, rf_out, rl_out, wrf2, rl2, ac2);
+            return;
+        }
         const double fn = fv[0], f1 = fv[1], f2 = fv[2];
         const double mu = cmu(gc);
         double g0, g1;
@@ -538,7 +564,8 @@ class SceneSolver {
 
     // ------------------------------------------------------------ Newton
     __device__ void newton(pdc_stats& st) {
-        const int n_rigid = 6 * n_local, n_force = 3 * nc, n_cons = 2 * nc;
+        const int n_rigid = 6 * n_local, n_force = (C.only_normal ? 1 : 3) * nc,
+                  n_cons = (C.only_normal ? 1 : 2) * nc;
         const bool direct = n_local < C.direct_threshold;
         double Hu = 1e-4, exitErr = 0;
         const double power = 0.66667;
@@ -551,12 +578,15 @@ class SceneSolver {
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 const double fn = B.f[3 * gc], f1 = B.f[3 * gc + 1], f2 = B.f[3 * gc + 2];
-                const double cn = -fn, cc = cone_c(fn, f1, f2, cmu(gc));
+                const double cn = -fn;
+                double cc = 0, g0 = 0, g1 = 0, h0 = 0, h1 = 0, h2 = 0;  // only_normal: c = -f_n alone
+                if (!C.only_normal) {
+                    cc = cone_c(fn, f1, f2, cmu(gc));
+                    cone_grad(f1, f2, g0, g1);
+                    cone_hess(f1, f2, h0, h1, h2);
+                }
                 B.cv[2 * gc] = cn;
                 B.cv[2 * gc + 1] = cc;
-                double g0, g1, h0, h1, h2;
-                cone_grad(f1, f2, g0, g1);
-                cone_hess(f1, f2, h0, h1, h2);
                 B.gr[2 * gc] = g0;
                 B.gr[2 * gc + 1] = g1;
                 B.hs[3 * gc] = h0;
@@ -599,8 +629,9 @@ class SceneSolver {
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 const double ln = B.lam[2 * gc], lt = B.lam[2 * gc + 1];
-                const double ic0 = 1. / (B.cv[2 * gc] - eps * ln);
-                const double ic1 = 1. / (B.cv[2 * gc + 1] - eps * lt);
+                // only_normal regularises c - eps (OnlyNormalForce.cpp:104), not c - eps lambda
+                const double ic0 = 1. / (B.cv[2 * gc] - eps * (C.only_normal ? 1.0 : ln));
+                const double ic1 = C.only_normal ? 0.0 : 1. / (B.cv[2 * gc + 1] - eps * lt);
                 B.invC[2 * gc] = ic0;
                 B.invC[2 * gc + 1] = ic1;
                 const double g0 = B.gr[2 * gc], g1 = B.gr[2 * gc + 1];
@@ -620,7 +651,8 @@ class SceneSolver {
                 const double k01 = 0 + a * g0 * g1 + lt * B.hs[3 * gc + 1];
                 const double k11 = eps + a * g1 * g1 + lt * B.hs[3 * gc + 2];
                 const double det = k00 * k11 - k01 * k01;
-                const double t00 = k11 / det, t01 = -k01 / det, t11 = k00 / det;
+                double t00 = k11 / det, t01 = -k01 / det, t11 = k00 / det;
+                if (C.only_normal) t00 = t01 = t11 = 0;  // no tangential block
                 B.ktInv[3 * gc] = t00;
                 B.ktInv[3 * gc + 1] = t01;
                 B.ktInv[3 * gc + 2] = t11;
@@ -1689,7 +1721,8 @@ class SceneSolver {
                 double rfv[3], rlv[2];
                 contact_residual_w(gc, R, w, fI, lI, muc, rfv, rlv, e[1], e[2], e[3]);
                 e[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
-                e[6] += (dlin[0] / lI[0]) * rlv[0] + (dlin[1] / lI[1]) * rlv[1];
+                e[6] += (dlin[0] / lI[0]) * rlv[0];
+                if (!C.only_normal) e[6] += (dlin[1] / lI[1]) * rlv[1];
             }
             T.sync();
             for (int i = tid; i < n_local; i += nt) {
@@ -1738,6 +1771,10 @@ class SceneSolver {
     __device__ __forceinline__ void contact_residual_w(int gc, const Frame& R, d3 w, const double* fv,
                                                        const double* lv, double muc, double* rfo, double* rlo,
                                                        double& wrf2, double& rl2, double& ac2) const {
+        if (C.only_normal) {
+            normal_residual(gc, R, w, fv[0], lv[0], muc, rfo, rlo, wrf2, rl2, ac2);
+            return;
+        }
         const double fn = fv[0], f1 = fv[1], f2 = fv[2];
         const double mu = cmu(gc);
         double g0, g1;
@@ -1780,7 +1817,7 @@ class SceneSolver {
             e[1] += rfv[0] * rfv[0] + rfv[1] * rfv[1] + rfv[2] * rfv[2];
             mx[0] = dmax(mx[0], dmax(fabs(rlv[0]), fabs(rlv[1])));
             const double fn = B.f[3 * gc];
-            mx[1] = dmax(mx[1], dmax(-fn, cone_c(fn, B.f[3 * gc + 1], B.f[3 * gc + 2], cmu(gc))));
+            mx[1] = dmax(mx[1], C.only_normal ? -fn : dmax(-fn, cone_c(fn, B.f[3 * gc + 1], B.f[3 * gc + 2], cmu(gc))));
             for (int k = 0; k < 3; ++k) B.lforce[3 * gc + k] = B.f[3 * gc + k] * cs * cm;
         }
         T.sync();
@@ -1795,7 +1832,7 @@ class SceneSolver {
         }
         T.sum(e);
         T.max(mx);
-        st.kkt_stationarity = dmax(sqrt(e[0]) / (6.0 * n_local), sqrt(e[1]) / (3.0 * nc));
+        st.kkt_stationarity = dmax(sqrt(e[0]) / (6.0 * n_local), sqrt(e[1]) / ((C.only_normal ? 1.0 : 3.0) * nc));
         st.kkt_complementarity = mx[0];
         st.kkt_cone = mx[1];
         st.char_mass = cm;

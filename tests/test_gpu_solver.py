@@ -100,6 +100,31 @@ def test_pair_mu_matches_oracle(gpu, seed):
     assert rel(np.concatenate([dv, da], 1), np.concatenate([odv, oda], 1), 0.0981) < 1e-9
 
 
+@pytest.mark.parametrize("restitution", [0.0, 0.5])
+@pytest.mark.parametrize("name", ["box_on_ground", "sphere", "columns", "stack10"])
+def test_only_normal_matches_oracle(gpu, name, restitution):
+    """OnlyNormalForce (1-D normal force, no friction) against the oracle's
+    restatement of it, single scenes and a batch."""
+    s, g = CASES[name]()
+    cfg = abi.default_config(tol=1e-8, force_model=abi.PDC_FORCE_ONLY_NORMAL, restitution=restitution)
+    out = gpu.Solver(cfg).solve(s, dt=0.01, gravity=g)
+    ora = oracle_lib.solve(s, gravity=g, cfg=cfg)
+    compare(out, ora)
+    assert np.all(out[2][:, 1:] == 0)  # no tangential impulse
+    assert out[3]["status"] == ora[3]["status"]
+
+
+def test_only_normal_batch_matches_oracle(gpu):
+    cfg = abi.default_config(tol=1e-8, force_model=abi.PDC_FORCE_ONLY_NORMAL, restitution=0.5)
+    sc = scenes.pile_batch(24, seed=77, n_min=4, n_max=128)
+    batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
+    dv, da, lf, st = gpu.Solver(cfg).batch_solve(batch)
+    odv, oda, olf, ost = oracle_lib.batch_solve(batch, cfg=cfg)
+    assert rel(lf, olf) < 1e-9
+    assert rel(np.concatenate([dv, da], 1), np.concatenate([odv, oda], 1), 0.0981) < 1e-9
+    assert [x["newton_iters"] for x in st] == pytest.approx([x["newton_iters"] for x in ost], abs=1)
+
+
 def test_known_answers_on_gpu(gpu):
     s = scenes.resting_box_stack(10)
     solver = gpu.Solver(abi.default_config(tol=1e-8))
