@@ -1,0 +1,141 @@
+"""Trajectory writer in the reference's output format (`FileSaver::saveToFile`,
+src/IO/FileSaver.cpp:137-206), for scenes stepped by the device world.
+
+`<name>.npz` holds `time` (float64 [frames]) and, per body i, `mesh_<i>`
+(float64 [frames + 1, 7]): row 0 is the render scale of the body's collision
+geometry (a box's half extents, a sphere's radius three times; Cube.cpp:62,
+Sphere.cpp:33) followed by four zeros, then one row per saved frame with the
+translation (x, y, z) and the rotation quaternion's coefficients (x, y, z, w)
+as Eigen's rotation-matrix conversion returns them.  Frames are saved after
+every `substeps` steps (SimulationSceneCLI.cpp:9-20).  `<name>.info` holds the
+timing summary text.  Planes (not a reference shape: the reference uses static
+boxes) get scale (1, 1, 1).
+"""
+import os
+import time as _time
+
+import numpy as np
+
+from . import abi
+
+
+def quat_to_matrix(q):
+    """Rotation matrices of unit quaternions q[..., (x, y, z, w)]."""
+    q = np.asarray(q, np.float64)
+    x, y, z, w = q[..., 0], q[..., 1], q[..., 2], q[..., 3]
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], -2)
+
+
+def quat_from_matrix(m):
+    """Quaternion (x, y, z, w) of a rotation matrix by Shepperd's method with the
+    branch order Eigen uses: the trace branch when trace > 0, else the largest
+    diagonal element (ties to the lower index), so the sign convention of the
+    reference's output is kept."""
+    m = np.asarray(m, np.float64)
+    q = np.zeros(4)
+    t = m[0, 0] + m[1, 1] + m[2, 2]
+    if t > 0:
+        s = np.sqrt(t + 1.0)
+        q[3] = 0.5 * s
+        s = 0.5 / s
+        q[0] = (m[2, 1] - m[1, 2]) * s
+        q[1] = (m[0, 2] - m[2, 0]) * s
+        q[2] = (m[1, 0] - m[0, 1]) * s
+    else:
+        i = 0
+        if m[1, 1] > m[0, 0]:
+            i = 1
+        if m[2, 2] > m[i, i]:
+            i = 2
+        j, k = (i + 1) % 3, (i + 2) % 3
+        s = np.sqrt(m[i, i] - m[j, j] - m[k, k] + 1.0)
+        q[i] = 0.5 * s
+        s = 0.5 / s
+        q[3] = (m[k, j] - m[j, k]) * s
+        q[j] = (m[j, i] + m[i, j]) * s
+        q[k] = (m[k, i] + m[i, k]) * s
+    return q
+
+
+def render_scale(shape_type, size):
+    if shape_type == abi.PDC_SHAPE_BOX:
+        return np.asarray(size, np.float64)[:3]
+    if shape_type == abi.PDC_SHAPE_SPHERE:
+        r = float(size[0])
+        return np.array([r, r, r])
+    return np.ones(3)
+
+
+class TrajectoryRecorder:
+    """Collects the saved frames of one scene (`record` after each frame) and
+    writes them in the reference's .npz/.info layout (`save`)."""
+
+    def __init__(self, scene):
+        self.types = np.asarray(scene["type"])
+        self.sizes = np.asarray(scene["size"], np.float64).reshape(-1, 3)
+        self.times = []
+        self.frames = []  # [frames][bodies][7]
+
+    def record(self, time, pos, quat):
+        pos = np.asarray(pos, np.float64).reshape(-1, 3)
+        rows = np.empty((pos.shape[0], 7))
+        rows[:, :3] = pos
+        R = quat_to_matrix(np.asarray(quat, np.float64).reshape(-1, 4))
+        for b in range(pos.shape[0]):
+            rows[b, 3:] = quat_from_matrix(R[b])
+        self.times.append(float(time))
+        self.frames.append(rows)
+
+    def arrays(self):
+        n = len(self.types)
+        out = {"time": np.asarray(self.times, np.float64)}
+        stack = np.stack(self.frames, 1) if self.frames else np.zeros((n, 0, 7))
+        for b in range(n):
+            a = np.zeros((len(self.frames) + 1, 7))
+            a[0, :3] = render_scale(int(self.types[b]), self.sizes[b])
+            a[1:] = stack[b]
+            out[f"mesh_{b}"] = a
+        return out
+
+    def save(self, path, info=""):
+        """Write `<path without extension>.npz` (stored, uncompressed entries) and
+        `<...>.info`; returns the two file names."""
+        base = os.path.splitext(path)[0]
+        np.savez(base + ".npz", **self.arrays())
+        with open(base + ".info", "w") as f:
+            f.write(info)
+        return base + ".npz", base + ".info"
+
+
+def bake(world, scene_index, frames, substeps, path, dt):
+    """Step `world` for `frames` frames of `substeps` steps each, saving scene
+    `scene_index` after every frame, and write the result files (the CLI's
+    baking loop, SimulationSceneCLI.cpp:9-20, then FileSaver)."""
+    sc = world.shapes.scenes[scene_index]
+    b0, b1 = int(world.shapes.body_offsets[scene_index]), int(world.shapes.body_offsets[scene_index + 1])
+    rec = TrajectoryRecorder(sc)
+    t = 0.0
+    wall = 0.0
+    contacts = 0
+    for _ in range(frames):
+        t0 = _time.perf_counter()
+        world.step(substeps)
+        world.sync()
+        wall += _time.perf_counter() - t0
+        t += substeps * dt
+        pos, quat, _, _ = world.state()
+        counts, _ = world.contacts()
+        contacts += int(counts[scene_index])
+        rec.record(t, pos[b0:b1], quat[b0:b1])
+    st, ov = world.stats()
+    s = st[scene_index]
+    n = max(frames, 1)
+    info = (f"Times per substep (seconds):\n\tTotal time: {wall / (n * substeps)}\n"
+            f"Average #contacts (after merge, last substep of each frame): {contacts / n}\n"
+            f"Average substeps per step: {substeps}\nTotal #solids: {b1 - b0}\n"
+            f"Last substep: Newton iterations {s['newton_iters']}, status {s['status']}, "
+            f"exit error {s['exit_err']:.6e}\n")
+    return rec.save(path, info)

@@ -98,3 +98,33 @@ def test_c1_ten_box_stack_settles():
     assert np.abs(pos[1:, :2]).max() < 1e-6
     assert st[0]["status"] == 0
     w.close()
+
+
+def test_bake_writes_reference_layout(tmp_path):
+    """The C1 stack baked for 20 frames of 10 substeps into the reference's
+    .npz/.info layout: every saved row is the world's pose after that frame
+    (a second world stepped in lockstep), quaternions as rotation-matrix
+    conversions of those poses."""
+    from primal_dual_contacts_miror_b200 import filesaver, lib
+
+    sc = scenes.stack_world(10, gap=0.001)
+    cfg = abi.default_config(tol=1e-8)
+    w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), cfg=cfg)
+    npz, info = filesaver.bake(w, 0, frames=20, substeps=10, path=str(tmp_path / "stack.gltf"), dt=0.01)
+    w.close()
+    d = np.load(npz)
+    assert d["time"].shape == (20,)
+    np.testing.assert_allclose(d["time"], 0.1 * np.arange(1, 21))
+    twin = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), cfg=cfg)
+    for f in range(20):
+        twin.step(10)
+        twin.sync()
+        pos, quat, _, _ = twin.state()
+        for b in range(len(sc["type"])):
+            row = d[f"mesh_{b}"][f + 1]
+            assert np.array_equal(row[:3], pos[b])
+            np.testing.assert_allclose(filesaver.quat_to_matrix(row[3:]), filesaver.quat_to_matrix(quat[b]),
+                                       atol=1e-14)
+    twin.close()
+    np.testing.assert_allclose(d["mesh_1"][0, :3], sc["size"][1])
+    assert "Total #solids: 11" in open(info).read()
