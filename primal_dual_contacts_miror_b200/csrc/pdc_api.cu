@@ -59,6 +59,8 @@ struct pdc_solver {
     // grid-wide solve of large scenes (cooperative launch)
     int grid_blocks = 0;
     int cluster_size = 0;  // CTAs of the cluster team (0: clusters unavailable)
+    unsigned int* d_cost = nullptr;  // per-scene solve time of the previous call (planner key)
+    int cost_cap = 0, cost_ns = -1;
     void* d_grid = nullptr;
     pdc::GridSync gsync;
     int* d_counter = nullptr;
@@ -218,6 +220,24 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
         s->arena.cap = cap;
     }
     carve(s->arena, ns, nb, nc, P, host_inputs, grid, dmax);
+    // scene cost history: kept while the batch has the same number of scenes
+    if (ns > s->cost_cap) {
+        if (s->d_cost) cudaFree(s->d_cost);
+        s->d_cost = nullptr;
+        s->cost_cap = 0;
+        cudaError_t e = cudaMalloc(&s->d_cost, std::max(ns, 1) * sizeof(unsigned int));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_fail(s, e, "cudaMalloc(scene costs)");
+        }
+        s->cost_cap = std::max(ns, 1);
+        s->cost_ns = -1;
+    }
+    if (ns != s->cost_ns) {
+        cudaError_t e = cudaMemset(s->d_cost, 0, std::max(ns, 1) * sizeof(unsigned int));
+        if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemset(scene costs)");
+        s->cost_ns = ns;
+    }
     return PDC_OK;
 }
 
@@ -355,6 +375,7 @@ extern "C" void pdc_destroy(pdc_solver* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->arena.base) cudaFree(s->arena.base);
     if (s->d_timers) cudaFree(s->d_timers);
+    if (s->d_cost) cudaFree(s->d_cost);
     if (s->d_counter) cudaFree(s->d_counter);
     if (s->d_grid) cudaFree(s->d_grid);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -378,6 +399,7 @@ extern "C" int pdc_reset(pdc_solver* s) {
 static int launch(pdc_solver* s, const pdc::BatchPtrs& P0, cudaStream_t st, const std::vector<int>* large = nullptr) {
     pdc::BatchPtrs P = P0;
     P.timers = s->d_timers;
+    P.cost = s->d_cost;
     if (P.n_scenes == 0) return PDC_OK;
     P.grid_large = (large && !large->empty() && s->cfg.grid_min_bodies > 0) ? 1 : 0;
     const int grid = grid_for(s, P.n_scenes);

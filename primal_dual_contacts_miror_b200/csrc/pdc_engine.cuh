@@ -87,6 +87,9 @@ struct BatchPtrs {
     int* inc_cnt;
     int* inc_cur;
     uint8_t* local;
+    // per scene: device time of its previous solve (ns; 0 = none), the planner's
+    // longest-first key.  Null unless the handle keeps a history.
+    unsigned int* cost = nullptr;
     int* lbody;    // the scene's local bodies (global index), ascending, in its body slice
     double* u;     // 6
     double* uold;  // 6
@@ -1211,7 +1214,9 @@ class SceneSolver {
 
     // Block Cholesky factorisation + solve of the Newton system: left-looking,
     // one elimination-tree level at a time (columns of a level are independent;
-    // one team sync per level in each of factor / forward / backward), so a pile
+    // one team sync per level in each of factor / forward / backward; a
+    // non-SPD pivot only marks the scene, read once after the factorisation --
+    // later columns then compute garbage in bounded loops), so a pile
     // of short stacks takes as many sequential steps as its tallest stack.
     // Stands in for the direct branch's SimplicialLDLT (:385-394).  Writes du;
     // false on a non-SPD pivot.
@@ -1263,13 +1268,12 @@ class SceneSolver {
                     }
                 }
             }
-            double fl[8] = {(double)bad, 0, 0, 0, 0, 0, 0, 0};
-            T.max(fl);  // also the level barrier
-            if (fl[0] > 0) {
-                bad = 1;
-                break;
-            }
-            T.sync();
+            T.sync();  // level barrier; a failed pivot is checked once after the factorisation
+        }
+        {
+            double fl[1] = {(double)bad};
+            T.max(fl);
+            bad = fl[0] > 0;
         }
         if (!bad) {
             for (int l = 0; l < nlev; ++l) {  // forward: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
@@ -1850,10 +1854,10 @@ class SceneSolver {
 // counts[0] = #CTA scenes, [1] = #warp scenes, [2] = CTA counter, [3] = warp counter.
 __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant__ BatchPtrs B,
                                                            const __grid_constant__ EngineCfg C) {
-    __shared__ int hist[2][32];
-    __shared__ int start[2][32];
+    __shared__ int hist[2][64];
+    __shared__ int start[2][64];
     const int ns = B.n_scenes;
-    if (threadIdx.x < 64) (&hist[0][0])[threadIdx.x] = 0;
+    if (threadIdx.x < 128) (&hist[0][0])[threadIdx.x] = 0;
     __syncthreads();
     auto size_of = [&](int s, int& nb, int& nc) {
         if (B.body_off) {
@@ -1868,18 +1872,30 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
         if (B.grid_large && C.grid_min_bodies > 0 && nb >= C.grid_min_bodies) return 2;  // host launches it
         return (nc <= C.warp_max_contacts && nb <= C.warp_max_bodies) ? 1 : 0;
     };
-    auto bucket_of = [&](int nc) { return 31 - min(31, 32 - __clz(nc + 1)); };  // large first
+    // longest first: the scene's previous solve time when known, else its
+    // contact count (the scenes of a stepped simulation change slowly); buckets
+    // of half an octave of the key, largest bucket first
+    auto key_of = [&](int s, int nc) {
+        const unsigned int c = B.cost ? B.cost[s] : 0u;
+        return (int)min(c ? c : (unsigned int)nc * 2048u, 0x7fffffffu);
+    };
+    auto bucket_of = [&](int key) {
+        const unsigned int k = (unsigned int)key + 1u;
+        const int p = 31 - __clz(k);                          // floor(log2 k), 0..31
+        const int half = (p > 0) ? (int)((k >> (p - 1)) & 1u) : 0;
+        return 63 - (2 * p + half);
+    };
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
         int nb, nc;
         size_of(s, nb, nc);
         const int q = queue_of(nb, nc);
-        if (q < 2) atomicAdd(&hist[q][bucket_of(nc)], 1);
+        if (q < 2) atomicAdd(&hist[q][bucket_of(key_of(s, nc))], 1);
     }
     __syncthreads();
     if (threadIdx.x < 2) {
         const int q = threadIdx.x;
         int acc = 0;
-        for (int b = 0; b < 32; ++b) {
+        for (int b = 0; b < 64; ++b) {
             start[q][b] = acc;
             acc += hist[q][b];
         }
@@ -1892,7 +1908,7 @@ __global__ void __launch_bounds__(1024) plan_scenes_kernel(const __grid_constant
         size_of(s, nb, nc);
         const int q = queue_of(nb, nc);
         if (q == 2) continue;  // large scene: solved by solve_scene_grid_kernel
-        const int pos = atomicAdd(&start[q][bucket_of(nc)], 1);
+        const int pos = atomicAdd(&start[q][bucket_of(key_of(s, nc))], 1);
         (q ? B.order_warp : B.order_cta)[pos] = s;
     }
 }
@@ -1921,6 +1937,10 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
         S.finish(st);
     } else {
         st.status = S.status;
+    }
+    if (T.rank == 0 && B.cost) {
+        const unsigned long long dtn = S.now() - t0;
+        B.cost[s] = (unsigned int)(dtn < 0xffffffffull ? (dtn ? dtn : 1ull) : 0xffffffffull);
     }
     if (T.rank == 0) {
         if (B.stats) B.stats[s] = st;
