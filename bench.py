@@ -341,6 +341,7 @@ def main():
     ap.add_argument("--pit-steps", type=int, default=200)
     ap.add_argument("--pile-steps", type=int, default=200)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--serve-rates", default="1000,5000,20000,50000")
     ap.add_argument("--serve-slots", type=int, default=2048)
     ap.add_argument("--serve-ticks", type=int, default=40)
@@ -367,11 +368,17 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg.device = local
-    solver = lib.Solver(cfg)
     batch = build_workload(args.scenes, rank_seed(rank))
     dev = lib.DeviceBatch(batch, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
+    tuning = None
+    if not args.no_tune:  # launch shape from the autotuner, timed on this batch before the timed region
+        from primal_dual_contacts_miror_b200 import autotune
+
+        cfg, table = autotune.tune(dev, cfg, torch, stream=stream)
+        tuning = {"chosen": table[0], "candidates": table}
+    solver = lib.Solver(cfg)
 
     def barrier():
         if world > 1:
@@ -430,12 +437,14 @@ def main():
         "config": {"workload": f"{args.scenes} box-pile scenes per GPU, 4-256 bodies log-uniform, plain FP64, "
                                f"tol {args.tol}, one persistent launch per step",
                    "contacts_per_gpu": int(a.n_contacts), "bodies_per_gpu": int(a.n_bodies),
-                   "sparse_max_bodies": args.sparse_max, "warp_max_contacts": args.warp_max_contacts,
-                   "warp_max_bodies": args.warp_max_bodies, "l2": "inputs larger than L2 (no flush)"},
+                   "sparse_max_bodies": args.sparse_max, "cta_threads": cfg.cta_threads,
+                   "warp_max_contacts": cfg.warp_max_contacts, "warp_max_bodies": cfg.warp_max_bodies,
+                   "l2": "inputs larger than L2 (no flush)"},
         "contact_newton_iters_per_s": ci * world / per_step_s,
         "newton_iters_mean": newton / len(stats),
         "scene_status": status_counts,
         "gpu_launches": 2 * args.steps,
+        "autotune": tuning,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if args.scenes == 4096 else None,
