@@ -61,6 +61,27 @@ def build(force=False, verbose=False, extra_flags=()):
     return LIB
 
 
+HOST_SRC = os.path.join(PKG, "host", "force_solver_host.cpp")
+HOST_BIN = os.path.join(LIBDIR, "force_solver_host")
+
+
+def build_host(force=False):
+    """Compile the C++ host program (the reference-side adapter over the C ABI),
+    linked against the in-tree libpdc.so.  Returns the executable's path."""
+    lib = build()
+    if (not force and os.path.exists(HOST_BIN) and os.path.getmtime(HOST_BIN) > os.path.getmtime(HOST_SRC)
+            and os.path.getmtime(HOST_BIN) > os.path.getmtime(lib)):
+        return HOST_BIN
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), HOST_SRC, "-o", HOST_BIN + ".tmp",
+           "-L", LIBDIR, "-lpdc", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    os.replace(HOST_BIN + ".tmp", HOST_BIN)
+    return HOST_BIN
+
+
 def build_oracle():
     """Compile the CPU oracle used by the tests and the CPU baseline."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)

@@ -162,3 +162,37 @@ baking:
     assert d["mesh_1"].shape == (101, 7)
     np.testing.assert_allclose(d["mesh_1"][-1, :3], [0, 0.5, 0], atol=2e-3)
     np.testing.assert_allclose(d["mesh_2"][-1, :3], [0, 1.5, 0], atol=4e-3)
+
+
+def test_cpp_host_adapter_matches_python_binding(tmp_path):
+    """The C++ host program packs reference-shaped records (poses, principal
+    inertia, contact positions and frames) as the ForceSolver adapter does and
+    calls pdc_solve; its velocity increments and impulses equal the Python
+    binding's solve of the same world scene."""
+    import subprocess
+
+    import host_io
+    from primal_dual_contacts_miror_b200 import build, lib
+
+    exe = build.build_host()
+    rng = np.random.default_rng(3)
+    sc = jumbled_scene(rng)
+    w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), contacts_per_body=24)
+    w.step(2)
+    hs = w.host_scene(0)
+    pos, quat, vel, ang = w.state()
+    counts, c = w.contacts()
+    w.close()
+    assert counts[0] > 10
+    inp, out = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    host_io.write_input(inp, 0.01, (0, 0, -9.81), pos, quat, vel, ang, sc["mass"], sc["inertia0"], sc["is_static"],
+                        c["body"], c["pos"], c["frame"], c["depth"])
+    r = subprocess.run([exe, inp, out, "100", "1e-8"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    status, iters, dv, dw, lf = host_io.read_output(out, len(sc["mass"]), int(counts[0]))
+    ref = lib.Solver(abi.default_config(tol=1e-8)).solve(hs)
+    scale = max(np.abs(ref[2]).max(), 1e-300)
+    assert np.abs(lf - ref[2]).max() / scale < 1e-9
+    v, rv = np.concatenate([dv, dw], 1), np.concatenate([ref[0], ref[1]], 1)
+    assert np.abs(v - rv).max() / max(np.abs(rv).max(), 0.0981) < 1e-9
+    assert status == ref[3]["status"] and abs(iters - ref[3]["newton_iters"]) <= 1
