@@ -284,7 +284,8 @@ void pdc_world_destroy(pdc_world* w);
 /* Enqueue n_steps steps on `stream` (a cudaStream_t; NULL = the legacy default
  * stream).  The step graph is captured on the first call. */
 int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream);
-/* Contact detection only, at the current poses (synchronous). */
+/* Contact detection only, at the current poses (synchronous: waits for all work
+   enqueued on the device, e.g. steps on the caller's stream). */
 int pdc_world_collide(pdc_world* w);
 /* Bounded wait for the world's work (PDC_ETIMEOUT after timeout_ms). */
 int pdc_world_sync(pdc_world* w, int32_t timeout_ms);

@@ -170,6 +170,7 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->cv = D(2 * nc);
     P->gr = D(2 * nc);
     P->hs = D(3 * nc);
+    P->tq = D(3 * nc);
     P->invC = D(2 * nc);
     P->knInv = D(nc);
     P->ktInv = D(3 * nc);

@@ -117,6 +117,7 @@ struct BatchPtrs {
     double* cv;     // 2 constraint values
     double* gr;     // 2 gradients
     double* hs;     // 3 hessian (packed)
+    double* tq;     // 3: tangential-weight form T_t^T M^-1 T_t of both bodies (packed 2x2)
     double* invC;   // 2
     double* knInv;  // 1
     double* ktInv;  // 3 (packed symmetric inverse of K_t)
@@ -442,6 +443,29 @@ class SceneSolver {
                 k += w.x * C.restitution;
             }
             B.kn[gc] = k;
+            {  // calculateTangentialWeight's mass term as a 2x2 form in the tangent direction
+                const Frame R = ld_frame(B.frame + 9 * gc);
+                const d3 t1 = from_frame(R, d3{0.0, 1.0, 0.0}), t2 = from_frame(R, d3{0.0, 0.0, 1.0});
+                double q00 = 0, q01 = 0, q11 = 0;
+                for (int j = 0; j < 2; ++j) {
+                    const int gb = b0 + B.cbody[2 * gc + j];
+                    if (B.is_static[gb]) continue;
+                    const d3 c = ld3(B.arm + 6 * gc + 3 * j);
+                    const d3 a = cross3(c, t1), e = cross3(c, t2);
+                    const double im = 1.0 / B.mass[gb];
+                    const double* J = B.inv_inertia + 6 * gb;
+                    const d3 Ja = d3{J[0] * a.x + J[3] * a.y + J[4] * a.z, J[3] * a.x + J[1] * a.y + J[5] * a.z,
+                                     J[4] * a.x + J[5] * a.y + J[2] * a.z};
+                    const d3 Je = d3{J[0] * e.x + J[3] * e.y + J[4] * e.z, J[3] * e.x + J[1] * e.y + J[5] * e.z,
+                                     J[4] * e.x + J[5] * e.y + J[2] * e.z};
+                    q00 += im * dot3(t1, t1) + dot3(a, Ja);
+                    q01 += im * dot3(t1, t2) + dot3(a, Je);
+                    q11 += im * dot3(t2, t2) + dot3(e, Je);
+                }
+                B.tq[3 * gc] = q00;
+                B.tq[3 * gc + 1] = q01;
+                B.tq[3 * gc + 2] = q11;
+            }
             B.f[3 * gc] = 1;
             B.f[3 * gc + 1] = 0;
             B.f[3 * gc + 2] = 0;
@@ -463,25 +487,16 @@ class SceneSolver {
     }
 
     // Tangential weight (calculateTangentialWeight, NonSmoothContactForce.cpp:74-104)
+    // The direction d = R (0, th0, th1) enters as hh_j = s_j [d; c_j x d], so the
+    // sum over the active bodies of hh_j^T M_j^-1 hh_j is th^T Q th with the
+    // per-contact Q = sum_j T_j,t^T M_j^-1 T_j,t computed once per solve (tq).
     __device__ __forceinline__ double tangential_weight(int gc, const Frame& R, d3 w, double fn) const {
+        (void)R;
         const double tn = sqrt(w.y * w.y + w.z * w.z);
         double th0 = w.y, th1 = w.z;
         if (tn > 0) { th0 = w.y / tn; th1 = w.z / tn; }
-        // world tangent direction d = R (0, th0, th1); hh_j = T_j[:,1:] th = s_j [d; c_j x d]
-        d3 d = from_frame(R, d3{0.0, th0, th1});
-        double fw = 0;
-        for (int j = 0; j < 2; ++j) {
-            const int gb = b0 + B.cbody[2 * gc + j];
-            if (B.is_static[gb]) continue;
-            d3 c = ld3(B.arm + 6 * gc + 3 * j);
-            d3 t = cross3(c, d);
-            const double im = 1.0 / B.mass[gb];
-            const double* J = B.inv_inertia + 6 * gb;
-            d3 Jt = d3{J[0] * t.x + J[3] * t.y + J[4] * t.z, J[3] * t.x + J[1] * t.y + J[5] * t.z,
-                       J[4] * t.x + J[5] * t.y + J[2] * t.z};
-            const double q = im * dot3(d, d) + dot3(t, Jt);
-            fw += q * cm;
-        }
+        const double* Q = B.tq + 3 * gc;
+        const double fw = (Q[0] * th0 * th0 + 2.0 * Q[1] * th0 * th1 + Q[2] * th1 * th1) * cm;
         const double rad = cone_radius(fn, cmu(gc));
         return dmin(rad / (tn + 1e-8) * fw, 1.0);
     }

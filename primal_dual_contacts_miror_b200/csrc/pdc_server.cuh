@@ -229,6 +229,7 @@ extern "C" int pdc_server_admit(pdc_server* v, const pdc_shapes_soa* sh, int32_t
         return fail(s, PDC_EBUSY, "contact pool full");
     }
     CK(cudaSetDevice(s->device), "cudaSetDevice");
+    CK(cudaDeviceSynchronize(), "server sync");  // a tick may be in flight on a non-blocking stream
     pdc::WorldPtrs& W = v->W;
     auto up = [&](const void* dst, const void* src, size_t bytes) {
         return cudaMemcpy(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice);

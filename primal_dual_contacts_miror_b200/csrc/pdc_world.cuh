@@ -457,6 +457,9 @@ extern "C" int pdc_world_collide(pdc_world* w) {
     if (!w) return PDC_EINVAL;
     pdc_solver* s = w->solver;
     CK(cudaSetDevice(s->device), "cudaSetDevice");
+    // steps may still be in flight on the caller's stream, which the world's own
+    // stream is not ordered after: collide from the poses they leave
+    CK(cudaDeviceSynchronize(), "world sync");
     int rc = world_collide(w, w->stream);
     if (rc) return rc;
     CK(cudaStreamSynchronize(w->stream), "collide");

@@ -176,14 +176,23 @@ def test_cpp_host_adapter_matches_python_binding(tmp_path):
 
     exe = build.build_host()
     rng = np.random.default_rng(3)
-    sc = jumbled_scene(rng)
+    sb = scenes.ShapeSceneBuilder()  # resting bodies of mixed sizes and orientations about z: converging solves
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    for k in range(6):
+        h = rng.uniform(0.1, 0.4, 3)
+        ang = rng.uniform(0, np.pi)
+        sb.add_box(tuple(h), (1.2 * k, 0.0, h[2] + 1e-4), quat=(0.0, 0.0, np.sin(ang / 2), np.cos(ang / 2)))
+    for k in range(3):
+        r = rng.uniform(0.1, 0.3)
+        sb.add_sphere(r, (1.2 * k, 2.0, r + 1e-4), vel=(0.5, 0.0, 0.0))
+    sc = sb.build()
     w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)), contacts_per_body=24)
-    w.step(2)
+    w.step(3)
     hs = w.host_scene(0)
     pos, quat, vel, ang = w.state()
     counts, c = w.contacts()
     w.close()
-    assert counts[0] > 10
+    assert counts[0] >= 27  # 4 per box, 1 per sphere
     inp, out = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
     host_io.write_input(inp, 0.01, (0, 0, -9.81), pos, quat, vel, ang, sc["mass"], sc["inertia0"], sc["is_static"],
                         c["body"], c["pos"], c["frame"], c["depth"])
@@ -191,8 +200,31 @@ def test_cpp_host_adapter_matches_python_binding(tmp_path):
     assert r.returncode == 0, r.stderr
     status, iters, dv, dw, lf = host_io.read_output(out, len(sc["mass"]), int(counts[0]))
     ref = lib.Solver(abi.default_config(tol=1e-8)).solve(hs)
+    assert status == ref[3]["status"] == 0, (status, ref[3])
     scale = max(np.abs(ref[2]).max(), 1e-300)
     assert np.abs(lf - ref[2]).max() / scale < 1e-9
     v, rv = np.concatenate([dv, dw], 1), np.concatenate([ref[0], ref[1]], 1)
     assert np.abs(v - rv).max() / max(np.abs(rv).max(), 0.0981) < 1e-9
-    assert status == ref[3]["status"] and abs(iters - ref[3]["newton_iters"]) <= 1
+    assert abs(iters - ref[3]["newton_iters"]) <= 1
+
+
+def test_collide_after_unsynchronised_step_sees_the_stepped_poses():
+    """pdc_world_collide right after pdc_world_step (no sync in between): the
+    contacts are built from the poses the step left (arm = point - center)."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    sb = scenes.ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    for k in range(8):
+        sb.add_sphere(0.2, (0.5 * k, 0.0, 0.2 - 1e-3), vel=(1.0, 0.0, 0.0))
+    sc = sb.build()
+    w = lib.World(abi.ShapeBatch([sc], 0.01, (0, 0, -9.81)))
+    for _ in range(5):
+        w.step(1)
+        w.collide()
+        pos, quat, vel, ang = w.state()
+        counts, c = w.contacts()
+        assert counts[0] == 8
+        arm = np.concatenate([c["pos"] - pos[c["body"][:, 0]], c["pos"] - pos[c["body"][:, 1]]], 1)
+        np.testing.assert_allclose(c["arm"][:, 3:], arm[:, 3:], atol=1e-12)
+    w.close()
