@@ -337,6 +337,13 @@ const char* pdc_last_error(const pdc_solver* s);
 /* Library version string. */
 const char* pdc_version(void);
 
+/* Page-locked host memory for the host-array calls (no counterpart in the
+ * reference): inputs and outputs of pdc_solve / pdc_batch_solve placed in it are
+ * copied by DMA at the link's full rate instead of through a staging copy.
+ * PDC_ENOMEM when the allocation fails, PDC_ENODEV without a device. */
+int pdc_host_alloc(size_t bytes, void** out);
+void pdc_host_free(void* p);
+
 #ifdef __cplusplus
 }
 #endif

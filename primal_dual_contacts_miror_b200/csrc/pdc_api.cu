@@ -690,6 +690,27 @@ extern "C" const char* pdc_last_error(const pdc_solver* s) {
 
 extern "C" const char* pdc_version(void) { return "pdc-b200 0.1 (sm_100a)"; }
 
+extern "C" int pdc_host_alloc(size_t bytes, void** out) {
+    if (!out) return PDC_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PDC_ENODEV;
+    }
+    cudaError_t e = cudaHostAlloc(out, std::max<size_t>(bytes, 1), cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return e == cudaErrorMemoryAllocation ? PDC_ENOMEM : PDC_ECUDA;
+    }
+    return PDC_OK;
+}
+
+extern "C" void pdc_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free single-scene solve.
 //

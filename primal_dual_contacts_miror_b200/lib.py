@@ -58,6 +58,10 @@ def load():
     lib.pdc_last_error.restype = C.c_char_p
     lib.pdc_version.argtypes = []
     lib.pdc_version.restype = C.c_char_p
+    lib.pdc_host_alloc.argtypes = [C.c_size_t, C.POINTER(vp)]
+    lib.pdc_host_alloc.restype = C.c_int
+    lib.pdc_host_free.argtypes = [vp]
+    lib.pdc_host_free.restype = None
     _lib = lib
     return lib
 
@@ -65,7 +69,44 @@ def load():
 EXPORTED_SYMBOLS = [
     "pdc_config_default", "pdc_create", "pdc_destroy", "pdc_reset", "pdc_solve", "pdc_solve_async",
     "pdc_batch_solve", "pdc_batch_solve_async", "pdc_sync", "pdc_timings", "pdc_last_error", "pdc_version",
+    "pdc_host_alloc", "pdc_host_free",
 ]
+
+
+def pinned_empty(shape, dtype=np.float64):
+    """Uninitialised numpy array in page-locked host memory (pdc_host_alloc),
+    freed when the array is garbage collected."""
+    import weakref
+
+    lib = load()
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape)) if shape else 1
+    p = C.c_void_p()
+    rc = lib.pdc_host_alloc(n * dtype.itemsize, C.byref(p))
+    if rc != abi.PDC_OK:
+        raise PdcError(rc, "pdc_host_alloc failed")
+    buf = (C.c_char * max(n * dtype.itemsize, 1)).from_address(p.value)
+    a = np.frombuffer(buf, dtype=dtype, count=n).reshape(shape)
+    weakref.finalize(buf, lib.pdc_host_free, p.value)
+    return a
+
+
+def pinned_copy(a):
+    out = pinned_empty(np.shape(a), np.asarray(a).dtype)
+    out[...] = a
+    return out
+
+
+def pin_batch(batch):
+    """Move a HostBatch's arrays into page-locked memory (in place; returns it)."""
+    s = batch.all
+    for name in ("vel", "ang_vel", "mass", "inertia", "inv_inertia", "is_static", "body", "frame", "arm", "depth"):
+        setattr(s, name, pinned_copy(getattr(s, name)))
+    if s.mu is not None:
+        s.mu = pinned_copy(s.mu)
+    for name in ("body_offsets", "contact_offsets", "dt", "gravity"):
+        setattr(batch, name, pinned_copy(getattr(batch, name)))
+    return batch
 
 
 class Solver:
@@ -105,10 +146,11 @@ class Solver:
         self._check(self.lib.pdc_solve(self.h, dt, g, C.byref(b), C.byref(c), C.byref(res)))
         return dvel, dang, lf, res.stats.as_dict()
 
-    def batch_solve(self, batch):
-        """All scenes of a HostBatch -> (dvel, dang_vel, local_force, [stats])."""
+    def batch_solve(self, batch, out=None):
+        """All scenes of a HostBatch -> (dvel, dang_vel, local_force, [stats]);
+        `out` = (dvel, dang_vel, local_force) arrays to fill (e.g. pinned)."""
         nb, nc = batch.all.n_bodies, batch.all.n_contacts
-        dvel, dang, lf = abi.result_arrays(nb, nc)
+        dvel, dang, lf = out if out is not None else abi.result_arrays(nb, nc)
         stats = (abi.Stats * max(batch.n_scenes, 1))()
         b = batch.all.bodies_struct()
         c = batch.all.contacts_struct()

@@ -46,6 +46,9 @@ def test_no_device_fails_loudly():
     with pytest.raises(lib.PdcError) as e:
         lib.Solver()
     assert e.value.code == abi.PDC_ENODEV
+    with pytest.raises(lib.PdcError) as e:
+        lib.pinned_empty((4, 3))
+    assert e.value.code == abi.PDC_ENODEV
 
 
 def test_config_defaults_match_reference_yaml_defaults():

@@ -125,6 +125,21 @@ def test_only_normal_batch_matches_oracle(gpu):
     assert [x["newton_iters"] for x in st] == pytest.approx([x["newton_iters"] for x in ost], abs=1)
 
 
+def test_pinned_host_buffers_give_the_same_result(gpu):
+    """pdc_batch_solve from page-locked inputs into page-locked outputs
+    (pdc_host_alloc) equals the same call on ordinary numpy arrays, bitwise."""
+    sc = scenes.pile_batch(32, seed=13, n_min=4, n_max=64)
+    cfg = abi.default_config(tol=1e-8)
+    plain = gpu.Solver(cfg).batch_solve(abi.HostBatch(sc, 0.01, (0, 0, -9.81)))
+    batch = gpu.pin_batch(abi.HostBatch(sc, 0.01, (0, 0, -9.81)))
+    a = batch.all
+    outs = (gpu.pinned_empty((a.n_bodies, 3)), gpu.pinned_empty((a.n_bodies, 3)), gpu.pinned_empty((a.n_contacts, 3)))
+    pinned = gpu.Solver(cfg).batch_solve(batch, out=outs)
+    for x, y in zip(plain[:3], pinned[:3]):
+        assert np.array_equal(x, y)
+    assert [s["newton_iters"] for s in plain[3]] == [s["newton_iters"] for s in pinned[3]]
+
+
 def test_known_answers_on_gpu(gpu):
     s = scenes.resting_box_stack(10)
     solver = gpu.Solver(abi.default_config(tol=1e-8))
