@@ -144,3 +144,36 @@ def test_ball_pit_world_steps():
     assert np.isfinite(pos).all() and np.isfinite(vel).all()
     assert pos[5:, 2].min() > -0.01  # nothing fell through the ground
     w.close()
+
+
+@pytest.mark.parametrize("team", sorted(TEAMS))
+def test_large_and_small_scenes_in_one_world(team):
+    """A world holding small scenes (block team) and one large scene (cluster or
+    whole GPU, sort-based collision): every scene's trajectory equals the same
+    scene stepped alone, bitwise -- the routing and the shared launches do not
+    couple scenes."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    kind, cmax = TEAMS[team]
+    rng = np.random.default_rng(21)
+    small = [scenes.box_drop_world(int(n), rng, height=2.0) for n in (3, 7, 12, 20)]
+    big = scenes.ball_pit_world(1200, np.random.default_rng(22), side=1.3)
+    mix = small[:2] + [big] + small[2:]
+    cfg = abi.default_config(tol=1e-6, cluster_max_contacts=cmax, cluster_max_bodies=BIG)
+    steps = 15
+    w = lib.World(abi.ShapeBatch(mix, 0.005, (0, 0, -9.81)), cfg=cfg)
+    w.step(steps)
+    w.sync()
+    pos_mix, _, vel_mix, _ = w.state()
+    st, ov = w.stats()
+    assert st[2]["team"] == kind and all(st[k]["team"] == 0 for k in (0, 1, 3, 4))
+    offs = np.concatenate([[0], np.cumsum([len(s["type"]) for s in mix])])
+    w.close()
+    for k, sc in enumerate(mix):
+        a = lib.World(abi.ShapeBatch([sc], 0.005, (0, 0, -9.81)), cfg=cfg)
+        a.step(steps)
+        a.sync()
+        pos, _, vel, _ = a.state()
+        a.close()
+        assert np.array_equal(pos, pos_mix[offs[k]:offs[k + 1]]), k
+        assert np.array_equal(vel, vel_mix[offs[k]:offs[k + 1]]), k
