@@ -125,6 +125,44 @@ def test_only_normal_batch_matches_oracle(gpu):
     assert [x["newton_iters"] for x in st] == pytest.approx([x["newton_iters"] for x in ost], abs=1)
 
 
+def _penetrating_scene(gpu):
+    """Boxes and spheres overlapping a ground plane by up to ~2 mm, with
+    velocities: a contact set with real depths (the spring model's input)."""
+    rng = np.random.default_rng(17)
+    sb = scenes.ShapeSceneBuilder()
+    sb.add_plane((0.0, 0.0, 0.0), "+z")
+    for k in range(5):
+        h = rng.uniform(0.1, 0.3, 3)
+        ang = rng.uniform(0, np.pi)
+        sb.add_box(tuple(h), (1.0 * k, 0.0, h[2] - rng.uniform(0, 2e-3)),
+                   quat=(0.0, 0.0, np.sin(ang / 2), np.cos(ang / 2)), vel=tuple(rng.normal(0, 0.2, 3)))
+    for k in range(4):
+        r = rng.uniform(0.1, 0.3)
+        sb.add_sphere(r, (1.0 * k, 1.5, r - rng.uniform(0, 2e-3)), vel=tuple(rng.normal(0, 0.2, 3)))
+    w = gpu.World(abi.ShapeBatch([sb.build()], 0.01, (0, 0, -9.81)))
+    hs = w.host_scene(0)
+    w.close()
+    assert hs.n_contacts >= 24 and hs.depth.max() > 1e-4
+    return hs
+
+
+@pytest.mark.parametrize("model", ["non_smooth_contact", "only_normal"])
+@pytest.mark.parametrize("variant", ["restitution0", "restitution05", "spring"])
+def test_force_variants_match_oracle(gpu, model, variant):
+    """The spring-based force (k from the penetration depth, compliance term)
+    and restitution (k from the approach velocity) of both force models
+    (NonSmoothContactForce.cpp:8-48, OnlyNormalForce.cpp:7-35) against the oracle."""
+    hs = _penetrating_scene(gpu)
+    kw = {"restitution0": dict(restitution=0.0), "restitution05": dict(restitution=0.5),
+          "spring": dict(spring_based=1, spring_k=1e5, spring_damp=0.01)}[variant]
+    fm = abi.PDC_FORCE_NON_SMOOTH_CONTACT if model == "non_smooth_contact" else abi.PDC_FORCE_ONLY_NORMAL
+    cfg = abi.default_config(tol=1e-8, force_model=fm, **kw)
+    out = gpu.Solver(cfg).solve(hs)
+    ora = oracle_lib.solve(hs, cfg=cfg)
+    compare(out, ora)
+    assert out[3]["status"] == ora[3]["status"]
+
+
 def test_pinned_host_buffers_give_the_same_result(gpu):
     """pdc_batch_solve from page-locked inputs into page-locked outputs
     (pdc_host_alloc) equals the same call on ordinary numpy arrays, bitwise."""
