@@ -284,6 +284,14 @@ void pdc_world_destroy(pdc_world* w);
 /* Enqueue n_steps steps on `stream` (a cudaStream_t; NULL = the legacy default
  * stream).  The step graph is captured on the first call. */
 int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream);
+/* n_steps steps with adaptive substeps (simulation.adaptive_timestep,
+   DynamicSystem.cpp:165-204): every scene advances by its full dt in substeps
+   min(1 - done, minLength / (2 (speed dt + 1e-8) substep_factor)), speed = the
+   largest AABB-corner speed about the mean corner velocity; at most
+   max_substeps per step.  Synchronous; substeps_out (may be NULL) = substeps run
+   (the most any scene needed, summed over the steps). */
+int pdc_world_step_adaptive(pdc_world* w, int32_t n_steps, double substep_factor, int32_t max_substeps,
+                            int32_t* substeps_out);
 /* Contact detection only, at the current poses (synchronous: waits for all work
    enqueued on the device, e.g. steps on the caller's stream). */
 int pdc_world_collide(pdc_world* w);

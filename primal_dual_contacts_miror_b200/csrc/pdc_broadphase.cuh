@@ -128,6 +128,11 @@ __global__ void large_total_kernel(const __grid_constant__ WorldPtrs W, LargeCol
     const int cap = W.contact_cap[scene + 1] - W.contact_cap[scene];
     const long long last = L.max_pairs - 1;
     const long long total = (long long)L.off[last] + L.cnt[last];
+    if (W.dt[scene] == 0.0) {  // done with its adaptive substeps
+        W.ccount[scene] = 0;
+        W.overflow[scene] = 0;
+        return;
+    }
     W.ccount[scene] = (int)min(total, (long long)cap);
     W.overflow[scene] = (int)max(0LL, total - cap) + *L.overflow;
 }

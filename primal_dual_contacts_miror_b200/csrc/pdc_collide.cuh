@@ -25,7 +25,7 @@ struct WorldPtrs {
     const int* body_cnt;      // optional [ns]: bodies of each slot (serving)
     const int* cap_cnt;       // optional [ns]: contact capacity of each slot
     const uint8_t* skip;      // optional [ns]: scenes collided by the sort-based path
-    const double* dt;         // [ns]
+    double* dt;               // [ns] (written by adaptive stepping)
     const double* grav;       // [ns][3]
     // shapes / state
     const int* type;

@@ -43,6 +43,13 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ Wo
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int s = blockIdx.x; s < W.n_scenes; s += gridDim.x) {
         if (W.skip && W.skip[s]) continue;  // large scene: sort-based path
+        if (W.dt[s] == 0.0) {  // scene done with its adaptive substeps: no contacts, no motion
+            if (tid == 0) {
+                W.ccount[s] = 0;
+                W.overflow[s] = 0;
+            }
+            continue;
+        }
         const int b0 = W.body_off[s], nb = W.body_cnt ? W.body_cnt[s] : W.body_off[s + 1] - b0;
         const int cap0 = W.contact_cap[s], cap = W.cap_cnt ? W.cap_cnt[s] : W.contact_cap[s + 1] - cap0;
         const long long npairs = (long long)nb * (nb - 1) / 2;
@@ -153,6 +160,98 @@ __global__ void integrate_kernel(const __grid_constant__ WorldPtrs W, const int*
     }
 }
 
+// Adaptive time stepping (DynamicSystem.cpp:165-204): one block per scene
+// computes its next substep.  Over the velocities of the 8 corners of every
+// body's axis-aligned box (RigidObjectBase.cpp:86-105; planes, not a
+// reference shape, count with their velocity only) it takes the componentwise min and max, their mean, and the largest
+// corner speed relative to that mean; the substep is min(1 - done,
+// minLength / (2 (speed T + 1e-8) factor)) of the full step T.  Scenes already
+// done get dt = 0 (no contacts, no motion).  *any is set while a scene moves.
+__global__ void __launch_bounds__(256) adaptive_substep_kernel(const __grid_constant__ WorldPtrs W,
+                                                               const double* __restrict__ dt_full, double* done,
+                                                               const double* __restrict__ min_len, double factor,
+                                                               int* any) {
+    __shared__ double s_red[6][8];
+    const int s = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    if (s >= W.n_scenes) return;
+    const double T = dt_full[s];
+    if (!(done[s] < 1.0)) {
+        if (tid == 0) W.dt[s] = 0.0;
+        return;
+    }
+    const int b0 = W.body_off[s], nb = W.body_off[s + 1] - b0;
+    auto corner_vel = [&](int gb, int c, d3 v, d3 w, const double* hs) {
+        const d3 off = d3{(c & 4) ? hs[0] : -hs[0], (c & 2) ? hs[1] : -hs[1], (c & 1) ? hs[2] : -hs[2]};
+        return sub3(v, cross3(off, w));  // vertVel = v - (corner - t) x w
+    };
+    auto half_sizes = [&](int gb, double* hs) {
+        const int type = W.type[gb];
+        if (type == SHAPE_SPHERE) {
+            hs[0] = hs[1] = hs[2] = W.size[3 * gb];
+        } else if (type == SHAPE_BOX) {
+            double R[9];
+            quat_to_R(W.quat + 4 * gb, R);
+            const double* h = W.size + 3 * gb;
+            for (int r = 0; r < 3; ++r) hs[r] = fabs(R[3 * r]) * h[0] + fabs(R[3 * r + 1]) * h[1] + fabs(R[3 * r + 2]) * h[2];
+        } else {
+            hs[0] = hs[1] = hs[2] = 0.0;
+        }
+    };
+    // pass 1: componentwise min / max of the corner velocities
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int b = tid; b < nb; b += blockDim.x) {
+        const int gb = b0 + b;
+        const d3 v = ld3(W.vel + 3 * gb), w = ld3(W.ang + 3 * gb);
+        double hs[3];
+        half_sizes(gb, hs);
+        for (int c = 0; c < 8; ++c) {
+            const d3 cv = corner_vel(gb, c, v, w, hs);
+            mn[0] = fmin(mn[0], cv.x); mn[1] = fmin(mn[1], cv.y); mn[2] = fmin(mn[2], cv.z);
+            mx[0] = fmax(mx[0], cv.x); mx[1] = fmax(mx[1], cv.y); mx[2] = fmax(mx[2], cv.z);
+        }
+    }
+    for (int k = 0; k < 3; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = fmin(mn[k], __shfl_down_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmax(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
+        }
+    if (lane == 0)
+        for (int k = 0; k < 3; ++k) { s_red[k][warp] = mn[k]; s_red[3 + k][warp] = mx[k]; }
+    __syncthreads();
+    double avg[3];
+    for (int k = 0; k < 3; ++k) {
+        double a = INFINITY, z = -INFINITY;
+        for (int i = 0; i < nw; ++i) { a = fmin(a, s_red[k][i]); z = fmax(z, s_red[3 + k][i]); }
+        avg[k] = 0.5 * (a + z);
+    }
+    __syncthreads();
+    // pass 2: largest corner speed relative to the mean
+    double sp = 0.0;
+    for (int b = tid; b < nb; b += blockDim.x) {
+        const int gb = b0 + b;
+        const d3 v = ld3(W.vel + 3 * gb), w = ld3(W.ang + 3 * gb);
+        double hs[3];
+        half_sizes(gb, hs);
+        for (int c = 0; c < 8; ++c) {
+            const d3 cv = corner_vel(gb, c, v, w, hs);
+            const d3 d = d3{cv.x - avg[0], cv.y - avg[1], cv.z - avg[2]};
+            sp = fmax(sp, sqrt(dot3(d, d)));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) sp = fmax(sp, __shfl_down_sync(0xffffffffu, sp, o));
+    if (lane == 0) s_red[0][warp] = sp;
+    __syncthreads();
+    if (tid == 0) {
+        double m = 0.0;
+        for (int i = 0; i < nw; ++i) m = fmax(m, s_red[0][i]);
+        double h = min_len[s] / (2 * (m * T + 1e-8) * factor);
+        h = fmin(1.0 - done[s], h);
+        W.dt[s] = h * T;
+        done[s] += h;
+        atomicOr(any, 1);
+    }
+}
+
 }  // namespace pdc
 
 // ------------------------------------------------------------------ host API
@@ -173,6 +272,11 @@ struct pdc_world {
     std::vector<int> large;  // scenes solved (and collided) by the whole GPU
     pdc::LargeCollide L;
     void* large_mem = nullptr;
+    // adaptive stepping: full step per scene, fraction done, minimum body length, flag
+    double* dt_full = nullptr;
+    double* done = nullptr;
+    double* min_len = nullptr;
+    int* flag = nullptr;
 };
 
 // Contact detection of every scene: one block per ordinary scene, the
@@ -298,6 +402,10 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
         w->body_scene = a.take<int>(nb);
         w->lforce = a.take<double>(3 * nc);
         w->stats = a.take<pdc_stats>(ns);
+        w->dt_full = a.take<double>(ns);
+        w->done = a.take<double>(ns);
+        w->min_len = a.take<double>(ns);
+        w->flag = a.take<int>(4);
         return a.off + 256;
     };
     const size_t need = carve_world(A);
@@ -314,6 +422,18 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
     up(W.body_off, body_offsets, (ns + 1) * sizeof(int));
     up(W.contact_cap, cap_off.data(), (ns + 1) * sizeof(int));
     up(W.dt, dt, ns * sizeof(double));
+    up(w->dt_full, dt, ns * sizeof(double));
+    {  // obbMinLength per scene: a box's shortest full side, a sphere's radius (Cube.cpp:66-70, Sphere.cpp:38-41)
+        std::vector<double> ml(ns, INFINITY);
+        for (int k = 0; k < n_scenes; ++k)
+            for (int b = body_offsets[k]; b < body_offsets[k + 1]; ++b) {
+                if (sh->type[b] == PDC_SHAPE_BOX)
+                    ml[k] = std::min(ml[k], 2.0 * std::min(sh->size[3 * b], std::min(sh->size[3 * b + 1], sh->size[3 * b + 2])));
+                else if (sh->type[b] == PDC_SHAPE_SPHERE)
+                    ml[k] = std::min(ml[k], sh->size[3 * b]);
+            }
+        up(w->min_len, ml.data(), ns * sizeof(double));
+    }
     up(W.grav, gravity, 3 * ns * sizeof(double));
     up(W.type, sh->type, nb * sizeof(int));
     up(W.size, sh->size, 3 * nb * sizeof(double));
@@ -451,6 +571,51 @@ extern "C" int pdc_world_step(pdc_world* w, int32_t n_steps, void* stream) {
     for (int k = 0; k < n_steps; ++k) CK(cudaGraphLaunch(w->exec, st), "graph launch");
     w->steps += n_steps;
     return PDC_OK;
+}
+
+// Steps with adaptive substeps (the reference's adaptive_timestep): each of the
+// n_steps steps advances every scene by its full dt in substeps sized by
+// adaptive_substep_kernel, each a contact detection + solve + integration
+// with the scene's substep dt.  Synchronous per substep (the host reads whether
+// any scene still moves); not captured in a graph.
+extern "C" int pdc_world_step_adaptive(pdc_world* w, int32_t n_steps, double substep_factor,
+                                       int32_t max_substeps, int32_t* substeps_out) {
+    if (!w) return PDC_EINVAL;
+    pdc_solver* s = w->solver;
+    if (n_steps < 0 || !(substep_factor > 0) || max_substeps <= 0)
+        return fail(s, PDC_EINVAL, "bad adaptive stepping arguments");
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    CK(cudaDeviceSynchronize(), "world sync");
+    cudaStream_t st = w->stream;
+    const int gb = std::max(1, std::min((w->nb + 255) / 256, s->num_sms * 8));
+    int total = 0, rc = PDC_OK;
+    for (int k = 0; k < n_steps && rc == PDC_OK; ++k) {
+        CK(cudaMemsetAsync(w->done, 0, w->ns * sizeof(double), st), "reset substeps");
+        int sub = 0;
+        for (; sub < max_substeps; ++sub) {
+            CK(cudaMemsetAsync(w->flag, 0, sizeof(int), st), "reset flag");
+            pdc::adaptive_substep_kernel<<<w->ns, 256, 0, st>>>(w->W, w->dt_full, w->done, w->min_len,
+                                                                  substep_factor, w->flag);
+            CK(cudaGetLastError(), "launch adaptive_substep_kernel");
+            int any = 0;
+            CK(cudaMemcpyAsync(&any, w->flag, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H flag");
+            CK(cudaStreamSynchronize(st), "adaptive sync");
+            if (!any) break;
+            rc = world_collide(w, st);
+            if (rc) break;
+            rc = launch(s, w->P, st, &w->large);
+            if (rc) break;
+            pdc::integrate_kernel<<<gb, 256, 0, st>>>(w->W, w->body_scene, w->nb);
+            CK(cudaGetLastError(), "launch integrate_kernel");
+        }
+        total += sub;
+    }
+    // the fixed-step path reads W.dt again
+    CK(cudaMemcpyAsync(w->W.dt, w->dt_full, w->ns * sizeof(double), cudaMemcpyDeviceToDevice, st), "restore dt");
+    CK(cudaStreamSynchronize(st), "adaptive sync");
+    w->steps += n_steps;
+    if (substeps_out) *substeps_out = total;
+    return rc;
 }
 
 extern "C" int pdc_world_collide(pdc_world* w) {

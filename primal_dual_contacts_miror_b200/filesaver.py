@@ -110,10 +110,11 @@ class TrajectoryRecorder:
         return base + ".npz", base + ".info"
 
 
-def bake(world, scene_index, frames, substeps, path, dt):
+def bake(world, scene_index, frames, substeps, path, dt, adaptive_factor=None):
     """Step `world` for `frames` frames of `substeps` steps each, saving scene
     `scene_index` after every frame, and write the result files (the CLI's
-    baking loop, SimulationSceneCLI.cpp:9-20, then FileSaver)."""
+    baking loop, SimulationSceneCLI.cpp:9-20, then FileSaver).  With
+    `adaptive_factor` every step is taken in adaptive substeps."""
     sc = world.shapes.scenes[scene_index]
     b0, b1 = int(world.shapes.body_offsets[scene_index]), int(world.shapes.body_offsets[scene_index + 1])
     rec = TrajectoryRecorder(sc)
@@ -122,7 +123,10 @@ def bake(world, scene_index, frames, substeps, path, dt):
     contacts = 0
     for _ in range(frames):
         t0 = _time.perf_counter()
-        world.step(substeps)
+        if adaptive_factor is not None:
+            world.step_adaptive(substeps, adaptive_factor)
+        else:
+            world.step(substeps)
         world.sync()
         wall += _time.perf_counter() - t0
         t += substeps * dt

@@ -204,6 +204,12 @@ class World:
     def step(self, n=1, stream=None):
         self._check(self.lib.pdc_world_step(self.h, n, C.c_void_p(stream or 0)))
 
+    def step_adaptive(self, n=1, substep_factor=10.0, max_substeps=1000):
+        """n steps with adaptive substeps (synchronous); returns the substeps run."""
+        out = C.c_int32()
+        self._check(self.lib.pdc_world_step_adaptive(self.h, n, substep_factor, max_substeps, C.byref(out)))
+        return out.value
+
     def sync(self, timeout_ms=600000):
         self._check(self.lib.pdc_world_sync(self.h, timeout_ms))
 
@@ -358,6 +364,8 @@ def _bind_world(lib):
     lib.pdc_world_destroy.restype = None
     lib.pdc_world_step.argtypes = [vp, C.c_int32, vp]
     lib.pdc_world_step.restype = C.c_int
+    lib.pdc_world_step_adaptive.argtypes = [vp, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32)]
+    lib.pdc_world_step_adaptive.restype = C.c_int
     lib.pdc_world_collide.argtypes = [vp]
     lib.pdc_world_collide.restype = C.c_int
     lib.pdc_world_sync.argtypes = [vp, C.c_int32]

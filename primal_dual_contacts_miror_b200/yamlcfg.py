@@ -148,14 +148,13 @@ def run(scene_file, output_file, frames=None):
     sim = load_simulation(scene_file)
     if sim["backend"] != "gpu":
         raise ValueError("the device world runs the gpu backend only")
-    if sim["adaptive_timestep"]:
-        raise ValueError("adaptive_timestep is not supported by the device world")
     sc = load_scene(scene_file)
     dt = sim["timestep"]
     n = frames if frames is not None else frames_to_bake(sim["baking_time"], dt)
     w = lib.World(abi.ShapeBatch([sc], dt, sim["gravity"]), cfg=sim["cfg"])
     try:
-        return filesaver.bake(w, 0, n, 1, output_file, dt)
+        return filesaver.bake(w, 0, n, 1, output_file, dt,
+                              adaptive_factor=sim["substep_factor"] if sim["adaptive_timestep"] else None)
     finally:
         w.close()
 

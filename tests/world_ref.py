@@ -40,6 +40,56 @@ def step(sc, state, dt, gravity, cfg):
     return st, contacts
 
 
+def min_length(sc):
+    """obbMinLength over the scene (Cube.cpp:66-70: shortest full side;
+    Sphere.cpp:38-41: radius); planes do not count."""
+    ml = np.inf
+    for t, s in zip(sc["type"], sc["size"]):
+        if t == 0:
+            ml = min(ml, 2.0 * min(s))
+        elif t == 1:
+            ml = min(ml, s[0])
+    return ml
+
+
+def aabb_half(t, size, quat):
+    if t == 1:
+        return np.full(3, size[0])
+    if t == 0:
+        return np.abs(npr.quat_to_R(quat)) @ np.asarray(size, float)
+    return np.zeros(3)
+
+
+def substep(sc, state, T, done, factor):
+    """Next substep fraction (DynamicSystem.cpp:165-193): corner velocities of
+    every body's axis-aligned box (RigidObjectBase.cpp:86-105), their
+    componentwise mid-range, the largest speed about it."""
+    pos, quat, vel, ang = state
+    corners = []
+    for b in range(len(pos)):
+        hs = aabb_half(sc["type"][b], sc["size"][b], quat[b])
+        for c in range(8):
+            off = np.array([hs[0] if c & 4 else -hs[0], hs[1] if c & 2 else -hs[1], hs[2] if c & 1 else -hs[2]])
+            corners.append(vel[b] - np.cross(off, ang[b]))
+    corners = np.array(corners)
+    avg = 0.5 * (corners.min(0) + corners.max(0))
+    speed = np.sqrt(((corners - avg) ** 2).sum(1)).max()
+    h = min_length(sc) / (2 * (speed * T + 1e-8) * factor)
+    return min(1.0 - done, h)
+
+
+def step_adaptive(sc, state, T, gravity, cfg, factor):
+    """One adaptive step: substeps of contact detection + solve + integration
+    until the whole step T is covered (DynamicSystem.cpp:165-204)."""
+    done, n = 0.0, 0
+    while done < 1.0:
+        h = substep(sc, state, T, done, factor)
+        step(sc, state, h * T, gravity, cfg)
+        done += h
+        n += 1
+    return n
+
+
 def initial_state(sc):
     return (np.array(sc["pos"], float).copy(), np.array(sc["quat"], float).copy(),
             np.array(sc["vel"], float).copy(), np.array(sc["ang_vel"], float).copy())
