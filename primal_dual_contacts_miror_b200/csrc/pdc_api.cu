@@ -475,12 +475,21 @@ static int validate_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies
         const int nb = batch->body_offsets[k + 1] - batch->body_offsets[k];
         const int c0 = batch->contact_offsets[k], c1 = batch->contact_offsets[k + 1];
         if (nb < 0 || c1 < c0) return fail(s, PDC_EINVAL, "non-monotone batch offsets");
-        for (int q = c0; q < c1; ++q)
+        if (!(batch->dt[k] > 0)) return fail(s, PDC_EINVAL, "time step must be positive");
+    }
+    return PDC_OK;
+}
+
+// Contact body ids inside their scene (the per-contact part of the checks;
+// run while the input copies are in flight).
+static int validate_ids(pdc_solver* s, const pdc_batch* batch, const pdc_contacts_soa* c) {
+    for (int k = 0; k < batch->n_scenes; ++k) {
+        const int nb = batch->body_offsets[k + 1] - batch->body_offsets[k];
+        for (int q = batch->contact_offsets[k]; q < batch->contact_offsets[k + 1]; ++q)
             for (int j = 0; j < 2; ++j) {
                 const int id = c->body[2 * q + j];
                 if (id < 0 || id >= nb) return fail(s, PDC_EINVAL, "contact body id out of range");
             }
-        if (!(batch->dt[k] > 0)) return fail(s, PDC_EINVAL, "time step must be positive");
     }
     return PDC_OK;
 }
@@ -525,6 +534,11 @@ static int batch_host(pdc_solver* s, const pdc_batch* batch, const pdc_bodies_so
         else P.cmu = nullptr;
     } else {
         P.cmu = nullptr;
+    }
+    rc = validate_ids(s, batch, c);  // on the host while the copies run
+    if (rc) {
+        cudaStreamSynchronize(st);  // the caller's buffers are read until the copies end
+        return rc;
     }
     const std::vector<int> large = large_scenes(s, ns, batch->body_offsets);
     rc = launch(s, P, st, &large);
