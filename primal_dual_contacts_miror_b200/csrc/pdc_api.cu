@@ -171,6 +171,8 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->gr = D(2 * nc);
     P->hs = D(3 * nc);
     P->tq = D(3 * nc);
+    P->wu = D(3 * nc);
+    P->wd = D(3 * nc);
     P->invC = D(2 * nc);
     P->knInv = D(nc);
     P->ktInv = D(3 * nc);

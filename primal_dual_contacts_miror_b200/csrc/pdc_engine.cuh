@@ -118,6 +118,8 @@ struct BatchPtrs {
     double* gr;     // 2 gradients
     double* hs;     // 3 hessian (packed)
     double* tq;     // 3: tangential-weight form T_t^T M^-1 T_t of both bodies (packed 2x2)
+    double* wu;     // 3: relative velocity J u at the iterate (line-search base)
+    double* wd;     // 3: J du of the search direction
     double* invC;   // 2
     double* knInv;  // 1
     double* ktInv;  // 3 (packed symmetric inverse of K_t)
@@ -529,6 +531,7 @@ class SceneSolver {
                                                      double& wrf2, double& rl2, double& ac2) const {
         const Frame R = ld_frame(B.frame + 9 * gc);
         const d3 w = rel_vel(gc, uvec);
+        st3(B.wu + 3 * gc, w);  // the line search steps from here: J(u + a du) = J u + a J du
         if (C.only_normal) {
             normal_residual(gc, R, w, fv[0], lv[0], muc, rf_out, rl_out, wrf2, rl2, ac2);
             return;
@@ -866,6 +869,7 @@ class SceneSolver {
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 const d3 w = rel_vel(gc, B.du);
+                st3(B.wd + 3 * gc, w);
                 double d0 = B.sf[3 * gc] - w.x, d1 = B.sf[3 * gc + 1] - w.y, d2 = B.sf[3 * gc + 2] - w.z;
                 d0 = B.knInv[gc] * d0;
                 const double t00 = B.ktInv[3 * gc], t01 = B.ktInv[3 * gc + 1], t11 = B.ktInv[3 * gc + 2];
@@ -897,6 +901,7 @@ class SceneSolver {
                 }
                 for (int c = tid; c < nc; c += nt) {
                     const int gc = c0 + c;
+                    st3(B.wd + 3 * gc, scl3(-1.0, rel_vel(gc, B.ru)));  // J du with du = -ru
                     for (int r = 0; r < 3; ++r) B.df[3 * gc + r] = B.rf[3 * gc + r];
                     B.dl[2 * gc] = B.rl[2 * gc];
                     B.dl[2 * gc + 1] = B.rl[2 * gc + 1];
@@ -1727,16 +1732,12 @@ class SceneSolver {
                 for (int k = 0; k < 3; ++k) fI[k] = __dadd_rn(B.f[3 * gc + k], __dmul_rn(0.99, dfin[k]));
                 for (int k = 0; k < 3; ++k) B.fT[3 * gc + k] = fI[k];
                 for (int k = 0; k < 2; ++k) B.lT[2 * gc + k] = lI[k];
-                // residual at the trial point with velocities u + 0.99 step du (both bodies)
+                // residual at the trial point u + 0.99 step du: J is linear, so its
+                // relative velocity is J u + 0.99 step J du (both stored per contact)
                 const Frame R = ld_frame(B.frame + 9 * gc);
-                d3 pv[2];
-                for (int j = 0; j < 2; ++j) {
-                    const int gb = b0 + B.cbody[2 * gc + j];
-                    double ui[6];
-                    trial_u(gb, step, ui);
-                    pv[j] = point_vel(ui, ld3(B.arm + 6 * gc + 3 * j));
-                }
-                const d3 w = to_frame(R, sub3(pv[1], pv[0]));
+                const double a = __dmul_rn(0.99, step);
+                const d3 wu = ld3(B.wu + 3 * gc), wd = ld3(B.wd + 3 * gc);
+                const d3 w = d3{fma(a, wd.x, wu.x), fma(a, wd.y, wu.y), fma(a, wd.z, wu.z)};
                 double rfv[3], rlv[2];
                 contact_residual_w(gc, R, w, fI, lI, muc, rfv, rlv, e[1], e[2], e[3]);
                 e[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
