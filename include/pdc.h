@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PDC_ABI_VERSION 1
+#define PDC_ABI_VERSION 2
 
 /* Call status codes. */
 enum pdc_status {
@@ -99,6 +99,8 @@ typedef struct pdc_config {
     int32_t sparse_max_bodies; /* direct branch: sparse block Cholesky on the device up to
                                   this many active bodies (256, the maximum); larger
                                   scenes use PCG */
+    int32_t sparse_max_bodies_large; /* the same for scenes solved by a thread-block cluster
+                                  or the whole GPU (2048, the maximum; 0 = PCG) */
     int32_t warp_max_contacts; /* batched launch: scenes with at most this many contacts */
     int32_t warp_max_bodies;   /* and bodies are solved by one warp, larger ones by a
                                   whole thread block (0 / 0 = blocks only, the default) */

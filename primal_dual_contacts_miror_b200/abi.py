@@ -7,7 +7,7 @@ import ctypes as C
 
 import numpy as np
 
-PDC_ABI_VERSION = 1
+PDC_ABI_VERSION = 2
 
 PDC_OK, PDC_EINVAL, PDC_ECUDA, PDC_ENOMEM, PDC_ETIMEOUT, PDC_ENODEV, PDC_EBUSY = range(7)
 STATUS_NAMES = {0: "PDC_OK", 1: "PDC_EINVAL", 2: "PDC_ECUDA", 3: "PDC_ENOMEM",
@@ -46,6 +46,7 @@ class Config(C.Structure):
         ("precision", C.c_int32),
         ("direct_threshold", C.c_int32),
         ("sparse_max_bodies", C.c_int32),
+        ("sparse_max_bodies_large", C.c_int32),
         ("warp_max_contacts", C.c_int32),
         ("warp_max_bodies", C.c_int32),
         ("cta_threads", C.c_int32),
@@ -205,6 +206,7 @@ def default_config(**overrides):
     cfg.precision = PDC_PRECISION_FP64
     cfg.direct_threshold = 2000
     cfg.sparse_max_bodies = 256
+    cfg.sparse_max_bodies_large = 2048
     cfg.warp_max_contacts = 0
     cfg.warp_max_bodies = 0
     cfg.cta_threads = 256

@@ -26,6 +26,8 @@ constexpr int kWarpsPerBlock = kThreads / 32;
 // sparse scratch: bitsets, orders, offsets, 2x256 diagonal blocks, 3 node vectors
 constexpr long long kSparseHeaderDoubles = 30720;
 constexpr long long kSparseBlocks = 3072;  // off-diagonal L blocks per scene
+// large-scene teams: index arrays, node blocks and kRowCapLarge off-diagonal blocks
+constexpr long long kSparseBigDoubles = pdc::kSparseLargeHeaderDoubles + 36LL * pdc::kRowCapLarge;
 
 struct Arena {
     void* base = nullptr;
@@ -60,6 +62,7 @@ struct pdc_solver {
     int grid_blocks = 0;
     int cluster_size = 0;  // CTAs of the cluster team (0: clusters unavailable)
     unsigned int* d_cost = nullptr;  // per-scene solve time of the previous call (planner key)
+    double* d_sparse_big = nullptr;  // sparse-factor slot of the large-scene teams
     int cost_cap = 0, cost_ns = -1;
     void* d_grid = nullptr;
     pdc::GridSync gsync;
@@ -97,6 +100,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.spring_damp = c.spring_damp;
     e.direct_threshold = c.direct_threshold;
     e.dense_max = c.sparse_max_bodies;
+    e.dense_max_large = c.sparse_max_bodies_large;
     e.warp_max_contacts = c.warp_max_contacts;
     e.warp_max_bodies = c.warp_max_bodies;
     e.grid_min_bodies = c.grid_min_bodies;
@@ -241,6 +245,18 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
         if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemset(scene costs)");
         s->cost_ns = ns;
     }
+    // sparse-factor slot of the large-scene teams, once a batch can hold a large scene
+    if (!s->d_sparse_big && s->cfg.grid_min_bodies > 0 && nb >= s->cfg.grid_min_bodies &&
+        s->cfg.sparse_max_bodies_large > 0) {
+        cudaError_t e = cudaMalloc(&s->d_sparse_big, kSparseBigDoubles * sizeof(double));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            s->d_sparse_big = nullptr;
+            return cuda_fail(s, e, "cudaMalloc(large-scene factor)");
+        }
+    }
+    P->sparse_big = s->d_sparse_big;
+    P->sparse_big_doubles = s->d_sparse_big ? kSparseBigDoubles : 0;
     return PDC_OK;
 }
 
@@ -262,6 +278,7 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->precision = PDC_PRECISION_FP64;
     c->direct_threshold = 2000;  // :385
     c->sparse_max_bodies = 256;
+    c->sparse_max_bodies_large = 2048;
     c->warp_max_contacts = 0;  // measured: thread blocks win even for small scenes
     c->warp_max_bodies = 0;
     c->cta_threads = 256;
@@ -292,6 +309,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
         return fail(s, PDC_EINVAL, "pcg_lanes not in {0, 1, 2, 4, 8}");
     if (c->sparse_max_bodies < 0 || c->sparse_max_bodies > pdc::kSparseMax)
         return fail(s, PDC_EINVAL, "sparse_max_bodies out of [0, 256]");
+    if (c->sparse_max_bodies_large < 0 || c->sparse_max_bodies_large > pdc::kSparseMaxLarge)
+        return fail(s, PDC_EINVAL, "sparse_max_bodies_large out of [0, 2048]");
     return PDC_OK;
 }
 
@@ -379,6 +398,7 @@ extern "C" void pdc_destroy(pdc_solver* s) {
     if (s->arena.base) cudaFree(s->arena.base);
     if (s->d_timers) cudaFree(s->d_timers);
     if (s->d_cost) cudaFree(s->d_cost);
+    if (s->d_sparse_big) cudaFree(s->d_sparse_big);
     if (s->d_counter) cudaFree(s->d_counter);
     if (s->d_grid) cudaFree(s->d_grid);
     if (s->stream) cudaStreamDestroy(s->stream);

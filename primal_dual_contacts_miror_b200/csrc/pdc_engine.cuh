@@ -37,6 +37,7 @@ struct EngineCfg {
     double spring_k, spring_damp;
     int direct_threshold;
     int dense_max;  // direct branch: sparse Cholesky up to this many active bodies (<= kSparseMax)
+    int dense_max_large;  // the same on the large-scene teams (<= kSparseMaxLarge)
     int warp_max_contacts;  // scenes up to this size are solved by one warp
     int warp_max_bodies;
     int grid_min_bodies;   // scenes with at least this many bodies are large
@@ -139,6 +140,9 @@ struct BatchPtrs {
     // per-team sparse-factorisation scratch (see SceneSolver::sparse_ws)
     double* dense;
     long long dense_stride;
+    // one slot for the large-scene teams (nullptr: they use PCG throughout)
+    double* sparse_big = nullptr;
+    long long sparse_big_doubles = 0;
     int* order_cta;   // scene queues written by plan_scenes_kernel
     int* order_warp;
     int* counts;      // [4]
@@ -147,10 +151,37 @@ struct BatchPtrs {
 
 #define PDC_STATUS_BAD_INPUT 16
 
-// sparse direct solve: nodes per scene (bitset width) 
+// sparse direct solve: nodes per scene (bitset width)
 constexpr int kSparseMax = 256;
 constexpr int kSparseWords = kSparseMax / 32;
 constexpr int kRowCap = 3072;  // off-diagonal factor blocks per scene
+
+// The large-scene teams (whole GPU, one cluster) solve one scene per launch and
+// factor up to kSparseMaxLarge active bodies: the whole direct branch, which
+// ends at 2,000 local bodies.  Their scratch is one slot of B.sparse_big.
+constexpr int kSparseMaxLarge = 2048;
+constexpr int kSparseWordsLarge = kSparseMaxLarge / 32;
+constexpr int kRowCapLarge = 1 << 16;
+// ints of the large slot's index arrays, before its double arrays
+constexpr long long kSparseLargeIntWords =
+    2LL * kSparseMaxLarge * kSparseWordsLarge + 12LL * (kSparseMaxLarge + 8) + 2LL * kRowCapLarge + 8;
+// doubles of the large slot before its off-diagonal blocks
+constexpr long long kSparseLargeHeaderDoubles = (kSparseLargeIntWords + 1) / 2 + 2LL * 36 * kSparseMaxLarge +
+                                                4LL * 6 * kSparseMaxLarge;
+// A large-team factor whose sequential depth exceeds kDirectDepthMax goes to
+// PCG instead.  Depth, in row updates (about 0.75 us each on one cluster): per
+// elimination level kLevelCost for the level's barrier and its chain of
+// dependent loads (about 10 us measured), plus the largest column's per-lane
+// row updates.  Contact graphs with short elimination trees (the stacks and
+// heaps of a filling pile) factor in well under a PCG solve's time (1.3-2 ms
+// per Newton step on these scenes); long strips and grid-like ones (a packed
+// crate, whose top separators are dense) do not.
+constexpr int kLevelCost = 14;
+constexpr int kDirectDepthMax = 2048;
+// Multiple minimum degree: a round eliminates independent nodes of degree up to
+// the minimum + kMmdDelta; past kMmdMaxRounds rounds the scene goes to PCG.
+constexpr int kMmdDelta = 2;
+constexpr int kMmdMaxRounds = 512;
 
 // W = R diag(kn, Kt^-1) R^T (packed symmetric)
 __device__ __forceinline__ void frame_sandwich(const Frame& R, double kni, double t00, double t01, double t11,
@@ -205,7 +236,16 @@ class SceneSolver {
     double compliance, reduction, spring_term;
     int n_local, n_active;
     bool dense_mode;
+    int sp_nw;  // bitset words in use (large teams)
     int status;
+    // sparse-factor capacities: the large-scene teams run one scene per launch
+    static constexpr bool kLargeTeam = Team::kind >= 2;
+    static constexpr int kSpMax = kLargeTeam ? kSparseMaxLarge : kSparseMax;
+    static constexpr int kSpWords = kSpMax / 32;  // bitset row stride
+    __device__ __forceinline__ int spw() const {
+        if constexpr (kLargeTeam) return sp_nw;
+        else return kSparseWords;
+    }
     unsigned long long t_build, t_solve, t_ls, t_mark;
 
     __device__ SceneSolver(const BatchPtrs& b, const EngineCfg& c, Team& t, int scene)
@@ -400,8 +440,12 @@ class SceneSolver {
         cs = csv;
         // sparse direct solve for scenes on the direct branch (the SimplicialLDLT
         // analogue, :385-394): compact node numbering + symbolic factorisation
-        dense_mode = !C.mixed && B.dense != nullptr && n_local < C.direct_threshold && C.dense_max > 0 &&
-                     n_active <= C.dense_max && n_active > 0 && C.dense_max <= kSparseMax;
+        {
+            const int dmax = kLargeTeam ? C.dense_max_large : C.dense_max;
+            const bool ws = kLargeTeam ? B.sparse_big != nullptr : B.dense != nullptr;
+            dense_mode = !C.mixed && ws && n_local < C.direct_threshold && dmax > 0 && n_active <= dmax &&
+                         n_active > 0 && dmax <= kSpMax;
+        }
         if (dense_mode) {
             T.scan(nb, 0, [&](int b) { return active(b0 + b) ? 1 : 0; },
                    [&](int b, int excl) {
@@ -410,7 +454,8 @@ class SceneSolver {
                            B.dbody[b0 + excl] = b0 + b;
                        }
                    });
-            dense_mode = sparse_symbolic();
+            if constexpr (kLargeTeam) dense_mode = sparse_symbolic_large();
+            else dense_mode = sparse_symbolic();
         }
         // velocities (non-dimensional) :203-217
         for (int i = tid; i < n_local; i += nt) {
@@ -957,8 +1002,48 @@ class SceneSolver {
         double* x;       // [kSparseMax][6]
         double* L;       // [cap][36] off-diagonal blocks, column by column
         int cap;
+        // large teams only
+        uint32_t* radj;  // [kSpMax][kSpWords] row patterns, bit k = column eliminated k-th
+        int* deg;        // current degree of each node; later the level cursors
+        int* sel;        // nodes eliminated in the current round
+        int* lvl_work;   // largest column work of each level
+        int* rowoff;     // [kRowCapLarge] block index of L(u, d) for each row-list entry
     };
     __device__ __forceinline__ Sparse sparse_ws() const {
+        if constexpr (kLargeTeam) {
+            constexpr int M = kSparseMaxLarge, M8 = kSparseMaxLarge + 8;
+            int* q = reinterpret_cast<int*>(B.sparse_big);
+            Sparse S;
+            S.adj = reinterpret_cast<uint32_t*>(q);
+            q += M * kSparseWordsLarge;
+            S.radj = reinterpret_cast<uint32_t*>(q);
+            q += M * kSparseWordsLarge;
+            S.perm = q; q += M8;
+            S.ipos = q; q += M8;
+            S.cstart = q; q += M8;
+            S.lvl_nodes = q; q += M8;
+            S.height = q; q += M8;
+            S.lvl_start = q; q += M8;
+            S.rowptr = q; q += M8;
+            S.deg = q; q += M8;
+            S.sel = q; q += M8;
+            S.lvl_work = q; q += M8;
+            q += 2 * M8;  // spare
+            S.rowidx = q; q += kRowCapLarge;
+            S.rowoff = q; q += kRowCapLarge;
+            S.meta = q;
+            double* d = B.sparse_big + (kSparseLargeIntWords + 1) / 2;
+            S.Dg = d; d += 36 * M;
+            S.Ld = d; d += 36 * M;
+            S.Ldi = d; d += 6 * M;
+            S.y = d; d += 6 * M;
+            S.z = d; d += 6 * M;
+            S.x = d; d += 6 * M;
+            S.L = d;
+            const long long left = B.sparse_big_doubles - kSparseLargeHeaderDoubles;
+            S.cap = left > 0 ? (int)min(left / 36, (long long)kRowCapLarge) : 0;
+            return S;
+        }
         char* p = reinterpret_cast<char*>(B.dense + (long long)T.slot * B.dense_stride);
         Sparse S;
         S.adj = reinterpret_cast<uint32_t*>(p);
@@ -1126,6 +1211,212 @@ class SceneSolver {
         return S.cstart[n] <= S.cap && S.cstart[n] <= kRowCap;
     }
 
+    // Symbolic factorisation on the large-scene teams (up to kSparseMaxLarge
+    // nodes), every step spread over the team.  Ordering: multiple minimum
+    // degree (Liu, ACM TOMS 11(2), 1985) -- each round eliminates the remaining
+    // nodes of degree at most the minimum + kMmdDelta that have no neighbour of
+    // that kind with a smaller (degree, node) key.  Those nodes are pairwise
+    // non-adjacent, so the round equals eliminating them one at a time (in node
+    // order); each remaining neighbour merges their patterns into its own and
+    // takes its elimination-tree height from them.
+    // Rows of the factor come from a transposed bitset indexed by elimination
+    // position, so every row list is in elimination order.  Returns false (PCG)
+    // if the factor does not fit the slot or its sequential depth is too large.
+    __device__ bool sparse_symbolic_large() {
+        Sparse S = sparse_ws();
+        const int n = n_active, nw = (n + 31) >> 5;
+        constexpr int W = kSpWords;
+        sp_nw = nw;
+        for (int q = tid; q < n * W; q += nt) {
+            S.adj[q] = 0;
+            S.radj[q] = 0;
+        }
+        for (int q = tid; q <= n; q += nt) {
+            S.ipos[q] = -1;
+            S.height[q] = 0;
+            S.lvl_start[q] = 0;
+            S.lvl_work[q] = 0;
+        }
+        T.sync();
+        for (int l = tid; l < n_local; l += nt) {  // node rows, each built by its owner
+            const int gb = B.lbody[b0 + l];
+            if (!active(gb)) continue;
+            const int i = B.didx[gb];
+            const int st0 = B.inc_start[gb], cnt = B.inc_cnt[gb];
+            for (int k = 0; k < cnt; ++k) {
+                const int e = B.inc[st0 + k];
+                const int go = b0 + B.cbody[2 * (e >> 1) + (1 - (e & 1))];
+                if (go == gb || !active(go)) continue;
+                const int j = B.didx[go];
+                S.adj[i * W + (j >> 5)] |= 1u << (j & 31);
+            }
+        }
+        T.sync();
+        for (int i = tid; i < n; i += nt) {
+            int d = 0;
+            for (int w = 0; w < nw; ++w) d += __popc(S.adj[i * W + w]);
+            S.deg[i] = d;
+        }
+        T.sync();
+        int done = 0;
+        for (int round = 0; round < kMmdMaxRounds; ++round) {
+            double m[1] = {-1e300};  // minimum degree over the remaining nodes
+            for (int i = tid; i < n; i += nt)
+                if (S.ipos[i] < 0) m[0] = dmax(m[0], -(double)S.deg[i]);
+            T.max(m);
+            if (m[0] < -1e299) break;  // all eliminated
+            const int dmin = (int)(-m[0]);
+            // candidates: degree <= dmin + kMmdDelta; a candidate is taken unless a
+            // neighbouring candidate has a smaller (degree, node) key
+            const int dcap = dmin + kMmdDelta;
+            for (int i = tid; i < n; i += nt) {
+                int pick = 0;
+                if (S.ipos[i] < 0 && S.deg[i] <= dcap) {
+                    pick = 1;
+                    const int ki = S.deg[i] * 65536 + i;
+                    const uint32_t* ai = S.adj + i * W;
+                    for (int w = 0; w < nw && pick; ++w) {
+                        uint32_t bits = ai[w];
+                        while (bits) {
+                            const int j = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (S.deg[j] <= dcap && S.deg[j] * 65536 + j < ki) {
+                                pick = 0;
+                                break;
+                            }
+                        }
+                    }
+                }
+                S.sel[i] = pick;
+            }
+            T.sync();
+            T.scan(n, done, [&](int i) { return S.sel[i]; },
+                   [&](int i, int excl) {
+                       if (S.sel[i]) {
+                           S.perm[excl] = i;
+                           S.ipos[i] = excl;
+                       }
+                   });
+            {
+                double c[1] = {0.0};  // nodes eliminated this round
+                for (int i = tid; i < n; i += nt) c[0] += S.sel[i];
+                T.sum(c);
+                done += (int)c[0];
+            }
+            for (int u = tid; u < n; u += nt) {  // remaining neighbours merge the eliminated patterns
+                if (S.ipos[u] >= 0) continue;
+                uint32_t* au = S.adj + u * W;
+                int h = S.height[u];
+                bool touched = false;
+                for (int w = 0; w < nw; ++w) {
+                    uint32_t bits = au[w];
+                    while (bits) {
+                        const int v = (w << 5) + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        if (!S.sel[v]) continue;
+                        touched = true;
+                        h = max(h, S.height[v] + 1);
+                        const uint32_t* av = S.adj + v * W;
+                        for (int x = 0; x < nw; ++x) au[x] |= av[x];
+                        au[w] &= ~(1u << (v & 31));
+                    }
+                }
+                if (touched) {
+                    au[u >> 5] &= ~(1u << (u & 31));
+                    int d = 0;
+                    for (int w = 0; w < nw; ++w) d += __popc(au[w]);
+                    S.deg[u] = d;
+                    S.height[u] = h;
+                }
+            }
+            T.sync();
+        }
+        if (done != n) return false;  // round limit
+        // block offsets in elimination order
+        T.scan(n, 0,
+               [&](int k) {
+                   int c = 0;
+                   for (int w = 0; w < nw; ++w) c += __popc(S.adj[S.perm[k] * W + w]);
+                   return c;
+               },
+               [&](int k, int excl) {
+                   S.cstart[S.perm[k]] = excl;
+                   if (k == n - 1) {
+                       int c = 0;
+                       for (int w = 0; w < nw; ++w) c += __popc(S.adj[S.perm[k] * W + w]);
+                       S.cstart[n] = excl + c;
+                   }
+               });
+        if (S.cstart[n] > S.cap || S.cstart[n] > kRowCapLarge) return false;
+        // row patterns: bit ipos(d) of row u for every u in pattern(d)
+        for (int d = tid; d < n; d += nt) {
+            const int kd = S.ipos[d];
+            const uint32_t* ad = S.adj + d * W;
+            for (int w = 0; w < nw; ++w) {
+                uint32_t bits = ad[w];
+                while (bits) {
+                    const int u = (w << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    atomicOr(&S.radj[u * W + (kd >> 5)], 1u << (kd & 31));
+                }
+            }
+        }
+        T.sync();
+        T.scan(n, 0,
+               [&](int u) {
+                   int c = 0;
+                   for (int w = 0; w < nw; ++w) c += __popc(S.radj[u * W + w]);
+                   return c;
+               },
+               [&](int u, int excl) {
+                   S.rowptr[u] = excl;
+                   if (u == n - 1) S.rowptr[n] = S.cstart[n];
+               });
+        // row lists in elimination order; levels by elimination-tree height
+        double hw[1] = {0.0};
+        for (int u = tid; u < n; u += nt) {
+            int a = S.rowptr[u];
+            for (int w = 0; w < nw; ++w) {
+                uint32_t bits = S.radj[u * W + w];
+                while (bits) {
+                    const int k = (w << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const int d = S.perm[k];
+                    S.rowidx[a] = d;
+                    S.rowoff[a++] = S.cstart[d] + bit_rank(S.adj + d * W, u);
+                }
+            }
+            atomicAdd(&S.lvl_start[S.height[u] + 1], 1);
+            hw[0] = dmax(hw[0], (double)S.height[u]);
+        }
+        T.max(hw);
+        const int nlev = (int)hw[0] + 1;
+        if (tid == 0) {
+            for (int l = 0; l < nlev; ++l) S.lvl_start[l + 1] += S.lvl_start[l];
+            S.meta[0] = nlev;
+        }
+        T.sync();
+        for (int l = tid; l < nlev; l += nt) S.deg[l] = S.lvl_start[l];  // level cursors
+        T.sync();
+        // Columns of a level are independent, so their order within the level
+        // changes no result.  Sequential work of column v as dense_solve_warp
+        // does it (one warp, lanes over the 6 (m + 1) block rows): each lane
+        // takes ceil(6 (m + 1) / 32) rows, each updated once per row-list entry;
+        // plus the level's fixed cost.
+        for (int v = tid; v < n; v += nt) {
+            S.lvl_nodes[atomicAdd(&S.deg[S.height[v]], 1)] = v;
+            int m = 0;
+            for (int w = 0; w < nw; ++w) m += __popc(S.adj[v * W + w]);
+            const int wk = kLevelCost + ((6 * (m + 1) + 31) >> 5) * (1 + S.rowptr[v + 1] - S.rowptr[v]);
+            atomicMax(&S.lvl_work[S.height[v]], wk);
+        }
+        T.sync();
+        double depth[1] = {0.0};
+        for (int l = tid; l < nlev; l += nt) depth[0] += S.lvl_work[l];
+        T.sum(depth);
+        return depth[0] <= kDirectDepthMax;
+    }
+
     // Column block of active body gb: the diagonal block P and, per incidence
     // with a body eliminated later, the off-diagonal block T_o K^-1 T_b^T
     // (linsysAddition's four blocks, :232-247).  Each column is owned by its
@@ -1136,9 +1427,9 @@ class SceneSolver {
         double* D = S.Dg + 36 * i;
         for (int r = 0; r < 6; ++r)
             for (int c = 0; c < 6; ++c) D[r * 6 + c] = P[pk(r, c)];
-        const uint32_t* ai = S.adj + i * kSparseWords;
+        const uint32_t* ai = S.adj + i * kSpWords;
         int m = 0;
-        for (int w = 0; w < kSparseWords; ++w) m += __popc(ai[w]);
+        for (int w = 0; w < spw(); ++w) m += __popc(ai[w]);
         double* col = S.L + 36LL * S.cstart[i];
         for (int q = 0; q < 36 * m; ++q) col[q] = 0.0;
         const int st0 = B.inc_start[gb], n = B.inc_cnt[gb];
@@ -1241,6 +1532,7 @@ class SceneSolver {
     // Stands in for the direct branch's SimplicialLDLT (:385-394).  Writes du;
     // false on a non-SPD pivot.
     __device__ bool dense_solve() {
+        if constexpr (kLargeTeam) return dense_solve_warp();
         Sparse S = sparse_ws();
         const int n = n_active;
         const int nlev = S.meta[0];
@@ -1248,18 +1540,18 @@ class SceneSolver {
         for (int l = 0; l < nlev; ++l) {
             for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
                 const int v = S.lvl_nodes[q];
-                const uint32_t* av = S.adj + v * kSparseWords;
+                const uint32_t* av = S.adj + v * kSpWords;
                 double* colv = S.L + 36LL * S.cstart[v];
                 double D[36];
                 for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
                 for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
                     const int d = S.rowidx[r];
-                    const uint32_t* ad = S.adj + d * kSparseWords;
+                    const uint32_t* ad = S.adj + d * kSpWords;
                     const double* cold = S.L + 36LL * S.cstart[d];
                     const double* Lvd = cold + 36 * bit_rank(ad, v);
                     sub_abt6(D, Lvd, Lvd);
                     int a = 0;  // walk pattern(d): u after v -> L(u,v) -= L(u,d) L(v,d)^T
-                    for (int w = 0; w < kSparseWords; ++w) {
+                    for (int w = 0; w < spw(); ++w) {
                         uint32_t bits = ad[w];
                         while (bits) {
                             const int u = (w << 5) + __ffs(bits) - 1;
@@ -1278,7 +1570,7 @@ class SceneSolver {
                 for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
                 for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
                 int m = 0;
-                for (int w = 0; w < kSparseWords; ++w) m += __popc(av[w]);
+                for (int w = 0; w < spw(); ++w) m += __popc(av[w]);
                 for (int a = 0; a < m; ++a) {  // L(u,v) = A(u,v) L_vv^-T, row by row
                     double* blk = colv + 36 * a;
                     for (int r = 0; r < 6; ++r) {
@@ -1304,7 +1596,7 @@ class SceneSolver {
                     for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r];
                     for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
                         const int d = S.rowidx[r];
-                        const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSparseWords, v));
+                        const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSpWords, v));
                         const double* yd = S.y + 6 * d;
                         for (int i = 0; i < 6; ++i) {
                             double t = 0.0;
@@ -1320,12 +1612,12 @@ class SceneSolver {
             for (int l = nlev - 1; l >= 0; --l) {  // backward: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
                 for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
                     const int v = S.lvl_nodes[q];
-                    const uint32_t* av = S.adj + v * kSparseWords;
+                    const uint32_t* av = S.adj + v * kSpWords;
                     const double* colv = S.L + 36LL * S.cstart[v];
                     double r6[6], xv[6];
                     for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r];
                     int a = 0;
-                    for (int w = 0; w < kSparseWords; ++w) {
+                    for (int w = 0; w < spw(); ++w) {
                         uint32_t bits = av[w];
                         while (bits) {
                             const int u = (w << 5) + __ffs(bits) - 1;
@@ -1349,6 +1641,170 @@ class SceneSolver {
             }
         }
         (void)n;
+        T.sync();
+        return !bad;
+    }
+
+    // node of the a-th set bit among the first nw words of a pattern
+    __device__ __forceinline__ static int bit_select_n(const uint32_t* w, int a, int nw) {
+        for (int k = 0; k < nw; ++k) {
+            const int c = __popc(w[k]);
+            if (a < c) {
+                uint32_t x = w[k];
+                for (int q = 0; q < a; ++q) x &= x - 1;
+                return (k << 5) + __ffs(x) - 1;
+            }
+            a -= c;
+        }
+        return -1;
+    }
+    __device__ __forceinline__ static void warp_sum6(double* s) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s[i] += __shfl_down_sync(0xffffffffu, s[i], o);
+    }
+
+    // The same factorisation and sweeps on the large-scene teams, which run one
+    // scene, so a level's time is its slowest column's chain of dependent loads:
+    // one warp per column (the level's columns strided over the team's warps).
+    // Lanes take the rows of the column's blocks -- row r of each L(u, v), u in
+    // pattern(v), and of the diagonal block -- and subtract their updates over
+    // the column's row list in elimination order, in place; lane 0 factors the
+    // diagonal block; then the lanes scale their rows by L_vv^-T, and the same
+    // warp does the column's forward substitution (its row list's columns are
+    // all in earlier levels), so one sweep over the levels factors and
+    // substitutes forward.  In the substitutions the lanes split a column's sum
+    // and combine it by a fixed shuffle tree.
+    __device__ bool dense_solve_warp() {
+        Sparse S = sparse_ws();
+        const int nlev = S.meta[0];
+        const int nw = spw();
+        const int lane = tid & 31, gwarp = tid >> 5, nwarp = nt >> 5;
+        int bad = 0;
+        for (int l = 0; l < nlev; ++l) {
+            for (int q = S.lvl_start[l] + gwarp; q < S.lvl_start[l + 1]; q += nwarp) {
+                const int v = S.lvl_nodes[q];
+                const uint32_t* av = S.adj + v * kSpWords;
+                double* colv = S.L + 36LL * S.cstart[v];
+                int m = 0;
+                for (int w = 0; w < nw; ++w) m += __popc(av[w]);
+                const int r0 = S.rowptr[v], r1 = S.rowptr[v + 1];
+                for (int t = lane; t < 6 * (m + 1); t += 32) {
+                    const int a = t / 6, r = t - 6 * a;
+                    const bool diag = a == m;
+                    const int u = diag ? v : bit_select_n(av, a, nw);
+                    double* dst = diag ? S.Dg + 36 * v + 6 * r : colv + 36 * a + 6 * r;
+                    double acc[6];
+                    for (int c = 0; c < 6; ++c) acc[c] = dst[c];
+                    for (int k = r0; k < r1; ++k) {
+                        const double* Lvd = S.L + 36LL * S.rowoff[k];
+                        const double* Lud = Lvd;
+                        if (!diag) {
+                            const int d = S.rowidx[k];
+                            const uint32_t* ad = S.adj + d * kSpWords;
+                            if (!((ad[u >> 5] >> (u & 31)) & 1u)) continue;
+                            Lud = S.L + 36LL * (S.cstart[d] + bit_rank(ad, u));
+                        }
+                        double x[6];
+                        for (int p = 0; p < 6; ++p) x[p] = Lud[6 * r + p];
+                        for (int c = 0; c < 6; ++c) {
+                            double s = 0.0;
+                            for (int p = 0; p < 6; ++p) s += x[p] * Lvd[6 * c + p];
+                            acc[c] -= s;
+                        }
+                    }
+                    for (int c = 0; c < 6; ++c) dst[c] = acc[c];
+                }
+                __syncwarp();
+                int ok = 0;
+                if (lane == 0) {
+                    double D[36], Lvv[36], Li[6];
+                    for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
+                    if (chol6(D, Lvv, Li)) {
+                        ok = 1;
+                        for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
+                        for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
+                    } else {
+                        bad = 1;
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                if (ok) {
+                    for (int t = lane; t < 6 * m; t += 32) {  // L(u,v) = A(u,v) L_vv^-T, row by row
+                        double* row = colv + 6 * t;
+                        double out[6];
+                        lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, row, out);
+                        for (int c = 0; c < 6; ++c) row[c] = out[c];
+                    }
+                    // forward substitution of this column (every d of its row list
+                    // is in an earlier level): y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
+                    double s6[6] = {0, 0, 0, 0, 0, 0};
+                    for (int k = r0 + lane; k < r1; k += 32) {
+                        const double* Lvd = S.L + 36LL * S.rowoff[k];
+                        const double* yd = S.y + 6 * S.rowidx[k];
+                        for (int i = 0; i < 6; ++i) {
+                            double t = 0.0;
+                            for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
+                            s6[i] += t;
+                        }
+                    }
+                    warp_sum6(s6);
+                    if (lane == 0) {
+                        const int gb = B.dbody[b0 + v];
+                        double b6[6], yv[6];
+                        for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r] - s6[r];
+                        lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
+                        for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
+                    }
+                }
+            }
+            T.sync();  // level barrier; a failed pivot is checked once after the factorisation
+        }
+        {
+            double fl[1] = {(double)bad};
+            T.max(fl);
+            bad = fl[0] > 0;
+        }
+        if (!bad) {
+            for (int l = nlev - 1; l >= 0; --l) {  // backward: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
+                for (int q = S.lvl_start[l] + gwarp; q < S.lvl_start[l + 1]; q += nwarp) {
+                    const int v = S.lvl_nodes[q];
+                    const uint32_t* av = S.adj + v * kSpWords;
+                    const double* colv = S.L + 36LL * S.cstart[v];
+                    double s6[6] = {0, 0, 0, 0, 0, 0};
+                    int a = 0;
+                    for (int w = 0; w < nw; ++w) {
+                        uint32_t bits = av[w];
+                        while (bits) {
+                            const int u = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if ((a & 31) == lane) {
+                                const double* blk = colv + 36 * a;
+                                const double* xu = S.x + 6 * u;
+                                for (int c = 0; c < 6; ++c) {
+                                    double t = 0.0;
+                                    for (int r = 0; r < 6; ++r) t += blk[6 * r + c] * xu[r];
+                                    s6[c] += t;
+                                }
+                            }
+                            ++a;
+                        }
+                    }
+                    warp_sum6(s6);
+                    if (lane == 0) {
+                        double r6[6], xv[6];
+                        for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r] - s6[r];
+                        ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
+                        for (int r = 0; r < 6; ++r) S.x[6 * v + r] = xv[r];
+                        const int gb = B.dbody[b0 + v];
+                        for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = xv[r];
+                    }
+                }
+                T.sync();
+            }
+        }
         T.sync();
         return !bad;
     }

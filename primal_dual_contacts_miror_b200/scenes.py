@@ -180,6 +180,64 @@ def settled_pile(n_boxes, rng, max_height=8, half_range=(0.05, 0.2), vel_noise=0
                      frame, arm, np.zeros(nc))
 
 
+def packed_lattice(nx, ny, nz, rng, half=0.1, vel_noise=0.01, density=1000.0):
+    """Contact set of an nx x ny x nz block of equal cubes packed face to face
+    on a static ground: 4 corner contacts per touching face pair, vertical and
+    lateral, so the contact graph is a 3-D grid (its sparse factor fills in,
+    unlike that of a pile of separate stacks).  Cube (i, j, k) is body
+    1 + i + nx (j + ny k); body 0 is the ground."""
+    from .geometry import frame_from_normal
+
+    n = nx * ny * nz
+    nb = n + 1
+    h = float(half)
+    gm, gi0 = box_mass_properties(GROUND_HALF, density)
+    m = density * (2 * h) ** 3
+    i0 = m / 12 * 2 * (2 * h) ** 2
+    mass = np.full(nb, m)
+    mass[0] = gm
+    inertia = np.zeros((nb, 6))
+    inertia[0, :3] = gi0
+    inertia[1:, :3] = i0
+    inv_inertia = np.zeros((nb, 6))
+    inv_inertia[:, :3] = 1.0 / inertia[:, :3]
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    pos = np.zeros((nb, 3))
+    pos[0] = (0, 0, -GROUND_HALF[2])
+    pos[1:] = np.stack([2 * h * i, 2 * h * j, h + 2 * h * k], 1)
+    vel = np.zeros((nb, 3))
+    ang = np.zeros((nb, 3))
+    vel[1:] = rng.normal(0, vel_noise, (n, 3))
+    ang[1:] = rng.normal(0, vel_noise, (n, 3))
+    is_static = np.zeros(nb, np.uint8)
+    is_static[0] = 1
+    idx = 1 + np.arange(n)
+    pairs, frames, points = [], [], []
+    s1 = np.array([-1, -1, 1, 1], float) * h
+    s2 = np.array([-1, 1, -1, 1], float) * h
+    for axis, ok, step in ((2, True, nx * ny), (0, i > 0, 1), (1, j > 0, nx)):
+        upper = idx if axis == 2 else idx[ok]
+        lower = np.where(k == 0, 0, idx - step) if axis == 2 else upper - step
+        c = pos[upper]
+        face = c.copy()
+        face[:, axis] -= h  # the face shared with the lower body
+        a, b = [q for q in range(3) if q != axis]
+        pts = np.repeat(face, 4, 0)
+        pts[:, a] += np.tile(s1, len(upper))
+        pts[:, b] += np.tile(s2, len(upper))
+        normal = np.zeros(3)
+        normal[axis] = 1.0
+        pairs.append(np.stack([np.repeat(lower, 4), np.repeat(upper, 4)], 1))
+        frames.append(np.tile(frame_from_normal(tuple(normal)).reshape(-1), (4 * len(upper), 1)))
+        points.append(pts)
+    body = np.concatenate(pairs).astype(np.int32)
+    cpos = np.concatenate(points)
+    arm = np.concatenate([cpos - pos[body[:, 0]], cpos - pos[body[:, 1]]], 1)
+    return HostScene(vel, ang, mass, inertia, inv_inertia, is_static, body, np.concatenate(frames), arm,
+                     np.zeros(len(body)))
+
+
 def pile_batch(n_scenes, seed, n_min=4, n_max=256, **kw):
     """Scenes with body counts log-uniform in [n_min, n_max] (the batched
     4096-scene workload's size distribution)."""

@@ -72,8 +72,8 @@ _ORACLE = {}
 @pytest.mark.parametrize("team", sorted(TEAMS))
 @pytest.mark.parametrize("n_boxes,tol,bar", [(1500, 1e-8, 1e-6), (2100, 1e-6, 1e-4)])
 def test_large_pile_matches_oracle(n_boxes, tol, bar, team):
-    """1,500 boxes: direct branch (PCG at 1e-13 on the GPU, LDL^T in the oracle),
-    Newton tolerance 1e-8.  2,100 boxes: iterative branch (block-Jacobi CG at
+    """1,500 boxes: direct branch (the large team's sparse block Cholesky on the
+    GPU, LDL^T in the oracle), Newton tolerance 1e-8.  2,100 boxes: iterative branch (block-Jacobi CG at
     1e-8, cap 1000, on both sides) at the default Newton tolerance 1e-6; the
     inexact CG directions trigger gradient-descent fall-backs on both sides, so
     the bar there is a small multiple of the Newton tolerance."""
@@ -93,7 +93,60 @@ def test_large_pile_matches_oracle(n_boxes, tol, bar, team):
     assert st["status"] == ost["status"] == 0
     assert st["team"] == kind
     assert st["n_local_bodies"] == n_boxes + 1
-    assert st["pcg_iters"] > 0
+    if n_boxes + 1 < 2000:
+        assert st["factor_blocks"] > 0 and st["pcg_iters"] == 0
+    else:
+        assert st["pcg_iters"] > 0 and st["factor_blocks"] == 0
+
+
+@pytest.mark.parametrize("team", sorted(TEAMS))
+@pytest.mark.parametrize("case", ["stacks700", "crate5x5x3", "crate6x6x2", "strip30x3", "strip100x3",
+                                  "crate10x10x3"])
+def test_large_team_sparse_factor(case, team):
+    """The large teams' own sparse factor (up to 2,048 active bodies, multiple
+    minimum degree order, a warp per column): stacks (a chain per column),
+    packed crates and strips of cubes (3-D and 2-D contact grids, whose factors
+    fill in) against the same team on PCG (sparse_max_bodies_large = 0) and the
+    oracle's LDL^T, and run against run bit for bit.  The 100x3 strip's
+    elimination tree (246 levels) and the 10x10x3 crate's dense top levels make
+    those factors too deep, and they go to PCG.  A crate's four
+    contacts per face pair make its impulses statically indeterminate: solvers
+    that differ in round-off end on different Newton paths (iteration counts,
+    impulse splits), so there the velocities are compared at the Newton
+    tolerance's scale."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    kind, cmax = TEAMS[team]
+    if case == "stacks700":
+        s = scenes.settled_pile(700, np.random.default_rng(1), vel_noise=0.01)
+    else:
+        dims = {"crate5x5x3": (5, 5, 3), "crate6x6x2": (6, 6, 2), "strip30x3": (30, 3, 1),
+                "strip100x3": (100, 3, 1), "crate10x10x3": (10, 10, 3)}[case]
+        s = scenes.packed_lattice(*dims, np.random.default_rng(10))
+    deep = case in ("strip100x3", "crate10x10x3")
+    kw = dict(tol=1e-8, grid_min_bodies=8, cluster_max_contacts=cmax, cluster_max_bodies=BIG)
+    solver = lib.Solver(abi.default_config(**kw))
+    d = solver.solve(s)
+    again = solver.solve(s)
+    p = lib.Solver(abi.default_config(sparse_max_bodies_large=0, **kw)).solve(s)
+    assert d[3]["team"] == p[3]["team"] == kind
+    if deep:
+        assert d[3]["factor_blocks"] == 0 and d[3]["pcg_iters"] > 0
+    else:
+        assert d[3]["factor_blocks"] > 0 and d[3]["pcg_iters"] == 0
+    assert p[3]["factor_blocks"] == 0 and p[3]["pcg_iters"] > 0
+    for a, b in zip(d[:3], again[:3]):
+        assert np.array_equal(a, b)
+    v = np.concatenate([d[0], d[1]], 1)
+    if case == "stacks700":
+        assert _rel(d[2], p[2]) < 1e-9
+        assert _rel(v, np.concatenate([p[0], p[1]], 1), 0.0981) < 1e-9
+        assert abs(d[3]["newton_iters"] - p[3]["newton_iters"]) <= 1
+    else:
+        assert _rel(v, np.concatenate([p[0], p[1]], 1), 0.0981) < 1e-6
+    odv, oda, olf, ost = oracle_lib.solve(s, cfg=abi.default_config(tol=1e-8), nthreads=8)
+    assert _rel(v, np.concatenate([odv, oda], 1), 0.0981) < 1e-6
+    assert d[3]["status"] == ost["status"] == 0
 
 
 def jumbled_large_scene(rng, n_box=500, n_sph=600, L=1.5, H=1.0):
