@@ -160,6 +160,7 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->rhs = D(6 * nb);
     P->ru = D(6 * nb);
     P->pinv = D(21 * nb);
+    P->dsc = D(6 * nb);
     P->inc = I(2 * nc);
     P->inc_o = I(2 * nc);
     P->f = D(3 * nc);

@@ -103,6 +103,7 @@ struct BatchPtrs {
     double* rhs;   // 6
     double* ru;    // 6
     double* pinv;  // 21
+    double* dsc;   // 6  Jacobi scale 1/sqrt(diag A) of the iterative branch
     // per-contact workspace
     int* inc;       // 2 per contact
     int* inc_o;     // 2 per contact: the incidence's other body (global index), -1 if static
@@ -731,7 +732,7 @@ class SceneSolver {
             }
             T.sync();
             // rhs = sum getTrans(j) K^-1 sf - ru; block-Jacobi blocks; PCG start
-            double rr[2] = {0, 0};  // r.z, b.b
+            double rr[3] = {0, 0, 0};  // r.z, b.b, |D b|^2 (iterative branch)
             for (int i = tid; i < n_local; i += nt) {
                 const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
@@ -776,6 +777,12 @@ class SceneSolver {
                     P[pk(3, 3)] += z0.x; P[pk(4, 3)] += z0.y; P[pk(4, 4)] += z1.y;
                     P[pk(5, 3)] += z0.z; P[pk(5, 4)] += z1.z; P[pk(5, 5)] += z2.z;
                 }
+                if (!direct)  // the reference solves the scaled system D A D (:359-376)
+                    for (int r = 0; r < 6; ++r) {
+                        const double d = 1 / sqrt(P[pk(r, r)]);
+                        B.dsc[6 * gb + r] = d;
+                        rr[2] += (d * rb[r]) * (d * rb[r]);
+                    }
                 if (dense_mode) {
                     assemble_dense_rows(gb, P);
                 } else {
@@ -791,6 +798,8 @@ class SceneSolver {
             }
             T.sum(rr);  // sync: rhs, pinv complete
             const double bnorm = sqrt(rr[1]);
+            // AMGCL's relative residual is measured in the scaled system: |D r| / |D b|
+            const double bn = direct ? bnorm : sqrt(rr[2]);
             unsigned long long t1 = now();
             t_build += t1 - t_mark;
             t_mark = t1;
@@ -810,7 +819,17 @@ class SceneSolver {
                 pcg_total += iters;
                 iters = conv ? 0 : maxit;  // the Hu rule sees a capped solve as maxCGIt
             } else {
-            if (!direct) {  // AMGCL starts from the previous du (:406-415)
+            if (!direct) {
+                // AMGCL starts from the previous du taken as the scaled unknown
+                // (:406-415), i.e. from D du here (this PCG runs on the unscaled
+                // system; with block-Jacobi preconditioning its iterates are the
+                // scaled PCG's times D); a zero right-hand side gives du = 0
+                for (int i = tid; i < n_local; i += nt) {
+                    const int gb = B.lbody[b0 + i];
+                    if (!active(gb)) continue;
+                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = bn > 0 ? B.dsc[6 * gb + r] * B.du[6 * gb + r] : 0.0;
+                }
+                T.sync();
                 spmv_to_X(B.du, nullptr, 0.0);
                 T.sync();
             }
@@ -833,14 +852,15 @@ class SceneSolver {
                     B.z[6 * gb + r] = z6[r];
                     B.p[6 * gb + r] = 0;
                     s2[0] += r6[r] * z6[r];
-                    s2[1] += r6[r] * r6[r];
+                    const double rs = direct ? r6[r] : B.dsc[6 * gb + r] * r6[r];
+                    s2[1] += rs * rs;
                 }
             }
             T.sum(s2);
             double rz = s2[0];
-            double res = (bnorm > 0) ? sqrt(s2[1]) / bnorm : 0.0;
+            double res = (bn > 0) ? sqrt(s2[1]) / bn : 0.0;
             double beta = 0;
-            if (bnorm == 0) {
+            if (bn == 0) {
                 // zero right-hand side: du = x0 (zero on the direct branch)
             } else if (!(res < rtol)) {
                 for (iters = 0; iters < maxit;) {
@@ -887,13 +907,14 @@ class SceneSolver {
                         prec(gb, r6, z6);
                         for (int r = 0; r < 6; ++r) {
                             B.z[6 * gb + r] = z6[r];
-                            s4[0] += r6[r] * r6[r];
+                            const double rs = direct ? r6[r] : B.dsc[6 * gb + r] * r6[r];
+                            s4[0] += rs * rs;
                             s4[1] += r6[r] * z6[r];
                         }
                     }
                     T.sum(s4);
                     ++iters;
-                    res = sqrt(s4[0]) / bnorm;
+                    res = sqrt(s4[0]) / bn;
                     if (!(res >= rtol)) break;  // converged or non-finite
                     beta = s4[1] / rz;
                     rz = s4[1];
