@@ -4,6 +4,7 @@ There is no CPU fallback: if the library is missing or no CUDA device is
 present, every entry point raises.
 """
 import ctypes as C
+from collections.abc import Sequence
 import os
 
 import numpy as np
@@ -18,6 +19,34 @@ class PdcError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
         self.code = code
+
+
+class SceneStats(Sequence):
+    """Per-scene statistics of a batched call, read-only: item k is scene k's
+    pdc_stats as a dict, converted when it is read (turning all of a 4,096-scene
+    batch's records into dicts on every call costs ~5 ms of Python)."""
+
+    def __init__(self, arr, n):
+        self._arr = arr
+        self._n = n
+
+    def __len__(self):
+        return self._n
+
+    def __getitem__(self, k):
+        if isinstance(k, slice):
+            return [self[i] for i in range(*k.indices(self._n))]
+        if k < 0:
+            k += self._n
+        if not 0 <= k < self._n:
+            raise IndexError(k)
+        return self._arr[k].as_dict()
+
+    def __eq__(self, other):
+        return list(self) == list(other)
+
+    def __repr__(self):
+        return f"SceneStats({list(self)!r})"
 
 
 def load():
@@ -147,8 +176,9 @@ class Solver:
         return dvel, dang, lf, res.stats.as_dict()
 
     def batch_solve(self, batch, out=None):
-        """All scenes of a HostBatch -> (dvel, dang_vel, local_force, [stats]);
-        `out` = (dvel, dang_vel, local_force) arrays to fill (e.g. pinned)."""
+        """All scenes of a HostBatch -> (dvel, dang_vel, local_force, stats), stats
+        a SceneStats (stats[k] = scene k's dict); `out` = (dvel, dang_vel,
+        local_force) arrays to fill (e.g. pinned)."""
         nb, nc = batch.all.n_bodies, batch.all.n_contacts
         dvel, dang, lf = out if out is not None else abi.result_arrays(nb, nc)
         stats = (abi.Stats * max(batch.n_scenes, 1))()
@@ -158,7 +188,7 @@ class Solver:
         dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
         self._check(self.lib.pdc_batch_solve(self.h, C.byref(bs), C.byref(b), C.byref(c), dp(dvel), dp(dang),
                                              dp(lf), stats))
-        return dvel, dang, lf, [stats[k].as_dict() for k in range(batch.n_scenes)]
+        return dvel, dang, lf, SceneStats(stats, batch.n_scenes)
 
     def batch_solve_device(self, dev, stream=None):
         """Enqueue a batched solve on device arrays.  `dev` is a DeviceBatch
