@@ -1236,13 +1236,24 @@ class SceneSolver {
     // nodes), every step spread over the team.  Ordering: multiple minimum
     // degree (Liu, ACM TOMS 11(2), 1985) -- each round eliminates the remaining
     // nodes of degree at most the minimum + kMmdDelta that have no neighbour of
-    // that kind with a smaller (degree, node) key.  Those nodes are pairwise
+    // that kind with a smaller key (mmd_key).  Those nodes are pairwise
     // non-adjacent, so the round equals eliminating them one at a time (in node
     // order); each remaining neighbour merges their patterns into its own and
     // takes its elimination-tree height from them.
     // Rows of the factor come from a transposed bitset indexed by elimination
     // position, so every row list is in elimination order.  Returns false (PCG)
     // if the factor does not fit the slot or its sequential depth is too large.
+    // Ordering key: degree, then a fixed hash of the node, then the node.  With
+    // the hash, independent equal-degree nodes along a chain or a strip leave in
+    // the same round, as in cyclic reduction, so a stack of L bodies gives an
+    // elimination tree of height ~log L instead of L / 2 (ends inward).
+    __device__ __forceinline__ static unsigned long long mmd_key(int deg, int i) {
+        unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return ((unsigned long long)deg << 32) | ((z >> 48) << 16) | (unsigned long long)i;
+    }
     __device__ bool sparse_symbolic_large() {
         Sparse S = sparse_ws();
         const int n = n_active, nw = (n + 31) >> 5;
@@ -1288,20 +1299,20 @@ class SceneSolver {
             if (m[0] < -1e299) break;  // all eliminated
             const int dmin = (int)(-m[0]);
             // candidates: degree <= dmin + kMmdDelta; a candidate is taken unless a
-            // neighbouring candidate has a smaller (degree, node) key
+            // neighbouring candidate has a smaller key
             const int dcap = dmin + kMmdDelta;
             for (int i = tid; i < n; i += nt) {
                 int pick = 0;
                 if (S.ipos[i] < 0 && S.deg[i] <= dcap) {
                     pick = 1;
-                    const int ki = S.deg[i] * 65536 + i;
+                    const unsigned long long ki = mmd_key(S.deg[i], i);
                     const uint32_t* ai = S.adj + i * W;
                     for (int w = 0; w < nw && pick; ++w) {
                         uint32_t bits = ai[w];
                         while (bits) {
                             const int j = (w << 5) + __ffs(bits) - 1;
                             bits &= bits - 1;
-                            if (S.deg[j] <= dcap && S.deg[j] * 65536 + j < ki) {
+                            if (S.deg[j] <= dcap && mmd_key(S.deg[j], j) < ki) {
                                 pick = 0;
                                 break;
                             }
