@@ -62,3 +62,23 @@ def test_config_defaults_match_reference_yaml_defaults():
     py = abi.default_config()
     for name, _ in abi.Config._fields_:
         assert getattr(py, name) == getattr(c, name), name
+
+
+def test_scene_stats_sequence_reads_each_scene_on_access():
+    """The batched call's per-scene statistics: a read-only sequence whose item
+    k is scene k's pdc_stats as a dict (index, negative index, slice,
+    iteration, equality with a list of dicts)."""
+    st = (abi.Stats * 4)()
+    for k in range(4):
+        st[k].newton_iters = 10 + k
+        st[k].team = k % 2
+    v = lib.SceneStats(st, 3)  # only the first three records belong to the call
+    assert len(v) == 3
+    assert v[0]["newton_iters"] == 10 and v[-1]["newton_iters"] == 12
+    assert [s["team"] for s in v] == [0, 1, 0]
+    assert [s["newton_iters"] for s in v[1:]] == [11, 12]
+    assert v == [st[k].as_dict() for k in range(3)]
+    with pytest.raises(IndexError):
+        v[3]
+    st[1].newton_iters = 99  # read when accessed: the dict reflects the record now
+    assert v[1]["newton_iters"] == 99
