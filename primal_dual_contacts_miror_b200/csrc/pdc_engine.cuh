@@ -346,7 +346,7 @@ class SceneSolver {
                 if (!B.is_static[b0 + b]) atomicAdd(&B.inc_cnt[b0 + b], 1);
             }
         }
-        double v[8] = {(double)bad, 0, 0, 0, 0, 0, 0, 0};
+        double v[1] = {(double)bad};
         T.max(v);
         if (v[0] > 0) { status |= PDC_STATUS_BAD_INPUT; return false; }
         // exclusive scan of counts -> absolute start in inc[]
@@ -400,7 +400,7 @@ class SceneSolver {
         }
         T.sync();
         // sort incidence lists, per-body speed, mass sums
-        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // n_local, n_active, traceSum, m*speed, m
+        double acc[5] = {0, 0, 0, 0, 0};  // n_local, n_active, traceSum, m*speed, m
         for (int b = tid; b < nb; b += nt) {
             const int gb = b0 + b;
             if (!B.local[gb]) continue;
@@ -641,7 +641,7 @@ class SceneSolver {
         for (it = 0; it < C.max_iter; ++it) {
             t_mark = now();
             // calculateConstraints (:105-118) + surrogateDualGap
-            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double acc[1] = {0};  // lambda . c
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 const double fn = B.f[3 * gc], f1 = B.f[3 * gc + 1], f2 = B.f[3 * gc + 2];
@@ -665,7 +665,7 @@ class SceneSolver {
             const double sDualGap = -(acc[0] / n_cons);
             const double muc = sDualGap * 0.1;
             // residuals at the current iterate (:292-300)
-            double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2
+            double e[4] = {0, 0, 0, 0};  // ru2, wrf2, rl2, ac2
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 contact_residual(gc, B.u, B.f + 3 * gc, B.lam + 2 * gc, true, muc, B.rf + 3 * gc, B.rl + 2 * gc,
@@ -1150,7 +1150,7 @@ class SceneSolver {
         T.sync();
         for (int k = 0; k < n; ++k) {
             // argmin (degree, node) over the remaining nodes
-            double best[8] = {-1e300, 0, 0, 0, 0, 0, 0, 0};
+            double best[1] = {-1e300};
             for (int i = tid; i < n; i += nt) {
                 if (S.ipos[i] >= 0) continue;
                 int d = 0;
@@ -1868,7 +1868,7 @@ class SceneSolver {
                 break;
             }
             // inner FP32 PCG on A e = r, e0 = 0
-            double s2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double s2[2] = {0, 0};
             for (int i = tid; i < n_local; i += nt) {
                 const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
@@ -1891,7 +1891,7 @@ class SceneSolver {
             for (int it = 0; it < C.max_direct && r0 > 0; ++it) {
                 spmv_to_Xf(beta);
                 T.sync();
-                double s3[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                double s3[1] = {0};
                 for (int i = tid; i < n_local; i += nt) {
                     const int gb = B.lbody[b0 + i];
                     if (!active(gb)) continue;
@@ -1910,7 +1910,7 @@ class SceneSolver {
                 }
                 T.sum(s3);
                 const float alpha = rz / (float)s3[0];
-                double s4[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                double s4[2] = {0, 0};
                 for (int i = tid; i < n_local; i += nt) {
                     const int gb = B.lbody[b0 + i];
                     if (!active(gb)) continue;
@@ -1945,7 +1945,7 @@ class SceneSolver {
             T.sync();
             spmv_to_X(B.du, nullptr, 0.0);
             T.sync();
-            double s5[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double s5[1] = {0};
             for (int i = tid; i < n_local; i += nt) {
                 const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
@@ -2211,7 +2211,7 @@ class SceneSolver {
         trials = 0;
         for (int t = 0; t < maxLS; ++t) {
             ++trials;
-            double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2, du.ru, df.rf, (dl/l).rl
+            double e[7] = {0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2, du.ru, df.rf, (dl/l).rl
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 double dfin[3], dlin[2], fI[3], lI[2];
@@ -2314,8 +2314,8 @@ class SceneSolver {
 
     // KKT report at the final iterate (mu_c = 0) and write-back (:491-510).
     __device__ void finish(pdc_stats& st) {
-        double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        double mx[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double e[2] = {0, 0};
+        double mx[2] = {0, 0};
         for (int c = tid; c < nc; c += nt) {
             const int gc = c0 + c;
             const Frame R = ld_frame(B.frame + 9 * gc);
