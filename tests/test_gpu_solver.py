@@ -257,6 +257,18 @@ def test_bad_body_id_is_einval(gpu):
     assert e.value.code == abi.PDC_EINVAL
 
 
+@pytest.mark.parametrize("field,value", [("sparse_max_bodies", 257), ("sparse_max_bodies", -1),
+                                         ("sparse_max_bodies_large", 2049), ("sparse_max_bodies_large", -1),
+                                         ("pcg_lanes", 3)])
+def test_config_out_of_range_is_einval(gpu, field, value):
+    """Sparse-factor limits beyond their scratch (256 on the block and warp
+    teams, 2,048 on the large-scene teams) and lane counts outside {0,1,2,4,8}
+    are configuration errors at creation."""
+    with pytest.raises(gpu.PdcError) as e:
+        gpu.Solver(abi.default_config(**{field: value}))
+    assert e.value.code == abi.PDC_EINVAL
+
+
 def test_iterative_branch_runs(gpu):
     s = scenes.resting_box_stack(6)
     cfg = abi.default_config(tol=1e-9, direct_threshold=1)
