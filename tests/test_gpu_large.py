@@ -4,6 +4,7 @@ detection against the per-scene all-pairs path."""
 import numpy as np
 import pytest
 
+import mmd_ref
 import oracle_lib
 from primal_dual_contacts_miror_b200 import abi, scenes
 
@@ -140,6 +141,8 @@ def test_large_team_sparse_factor(case, team):
         assert d[3]["factor_blocks"] == 0 and d[3]["pcg_iters"] > 0
     else:
         assert d[3]["factor_blocks"] > 0 and d[3]["pcg_iters"] == 0
+        # the device ordering and fill, block for block, against the restatement
+        assert d[3]["factor_blocks"] == mmd_ref.factor_blocks(mmd_ref.active_graph(s.body, s.is_static))
     assert p[3]["factor_blocks"] == 0 and p[3]["pcg_iters"] > 0
     for a, b in zip(d[:3], again[:3]):
         assert np.array_equal(a, b)
