@@ -1,7 +1,9 @@
-"""Restatement of the large-scene teams' symbolic factorisation (test
-infrastructure): the multiple-minimum-degree order with hashed ties that
-`SceneSolver::sparse_symbolic_large` (csrc/pdc_engine.cuh) computes on the
-device, and the sizes it reports.
+"""Restatement of the sparse factor's symbolic phase (test infrastructure):
+the multiple-minimum-degree order with hashed ties that the large-scene teams
+compute on the device (`SceneSolver::sparse_symbolic_large`,
+csrc/pdc_engine.cuh), the strict minimum-degree order of the block and warp
+teams (`SceneSolver::sparse_symbolic`, `symbolic_strict` below), and the sizes
+they report.
 
 Nodes are the scene's active bodies (not static, in at least one contact),
 numbered in body order; two nodes are adjacent when a contact joins them.  Each
@@ -89,3 +91,28 @@ def levels(adj):
     """Elimination-tree levels (the factor's sequential sweeps)."""
     _, _, height, _ = symbolic(adj)
     return max(height) + 1 if height else 0
+
+
+def symbolic_strict(adj):
+    """The block and warp teams' order (`SceneSolver::sparse_symbolic`): one
+    node per step, the remaining node of smallest (degree, node); returns the
+    elimination order and the column patterns."""
+    n = len(adj)
+    A = [set(s) for s in adj]
+    perm, pattern = [], {}
+    remaining = set(range(n))
+    while remaining:
+        v = min(remaining, key=lambda i: (len(A[i]), i))
+        perm.append(v)
+        pattern[v] = set(A[v])
+        remaining.discard(v)
+        for u in A[v]:
+            A[u] |= A[v]
+            A[u].discard(u)
+            A[u].discard(v)
+    return perm, pattern
+
+
+def factor_blocks_strict(adj):
+    _, pattern = symbolic_strict(adj)
+    return sum(len(p) for p in pattern.values())

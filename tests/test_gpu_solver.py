@@ -257,6 +257,20 @@ def test_bad_body_id_is_einval(gpu):
     assert e.value.code == abi.PDC_EINVAL
 
 
+def test_block_team_factor_matches_restated_order(gpu):
+    """The block team's sparse factor on 64 pile scenes of the headline's size
+    distribution: its off-diagonal block count equals that of the restated
+    strict minimum-degree order (tests/mmd_ref.py), scene by scene."""
+    import mmd_ref
+
+    sc = scenes.pile_batch(64, seed=29)
+    out = gpu.Solver(abi.default_config(tol=1e-8)).batch_solve(abi.HostBatch(sc, 0.01, (0, 0, -9.81)))
+    for k, s in enumerate(sc):
+        assert out[3][k]["team"] == 0
+        expect = mmd_ref.factor_blocks_strict(mmd_ref.active_graph(s.body, s.is_static))
+        assert out[3][k]["factor_blocks"] == expect, (k, out[3][k]["factor_blocks"], expect)
+
+
 @pytest.mark.parametrize("field,value", [("sparse_max_bodies", 257), ("sparse_max_bodies", -1),
                                          ("sparse_max_bodies_large", 2049), ("sparse_max_bodies_large", -1),
                                          ("pcg_lanes", 3)])

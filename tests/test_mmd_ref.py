@@ -63,3 +63,17 @@ def test_active_graph_of_a_pile():
     assert len(adj) == 40
     assert all(len(a) <= 2 for a in adj)
     check_symbolic(adj)
+
+
+def test_strict_order_is_a_valid_factorisation():
+    for adj in (chain(8), grid(6, 5), grid(12, 3)):
+        perm, pattern = mmd_ref.symbolic_strict(adj)
+        pos = {v: k for k, v in enumerate(perm)}
+        for v in range(len(adj)):
+            assert all(pos[u] > pos[v] for u in pattern[v])
+            assert {u for u in adj[v] if pos[u] > pos[v]} <= pattern[v]
+            if pattern[v]:
+                p = min(pattern[v], key=lambda u: pos[u])
+                assert pattern[v] - {p} <= pattern[p]
+    # ends first, lowest node first: a chain numbered in order is eliminated from node 0
+    assert mmd_ref.symbolic_strict(chain(8))[0] == list(range(8))
