@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PDC_ABI_VERSION 2
+#define PDC_ABI_VERSION 3
 
 /* Call status codes. */
 enum pdc_status {
@@ -122,6 +122,12 @@ typedef struct pdc_config {
     double mixed_inner_rtol;  /* FP32 inner PCG relative residual (mixed precision) */
     int32_t warm_start;       /* 0: cold start every step, as the reference (:269) */
     int32_t device;           /* CUDA device ordinal */
+    int32_t ls_max_trials;    /* line-search trials of a Newton step (10, lineSearch(..., 10) at
+                                 PrimalDualForceSolver.cpp:437-440) */
+    int32_t gd_max_trials;    /* line-search trials of the gradient-descent fallback (20, :454-456) */
+    int64_t barrier_timeout_us; /* bound on one wait at the whole-GPU team's grid barrier; when it
+                                 runs out every block of that launch ends at once and the call
+                                 returns PDC_ETIMEOUT (10,000,000 = 10 s; must be positive) */
 } pdc_config;
 
 /* Body state (input).  See the layout note at the top of this file. */
@@ -235,19 +241,26 @@ int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
  * captured), an engine that owns all device memory through its own pool or
  * budget, or a real-time loop that cannot afford an allocation's latency or
  * failure.  It needs no handle and calls no cudaMalloc/cudaFree: its scratch is
- * a fixed 2 MiB array inside the library (every GPU that loads the library holds
+ * a fixed 3 MiB array inside the library (every GPU that loads the library holds
  * it until exit).  Every pointer in bodies/contacts/out is a DEVICE pointer the
  * caller owns (is_static and depth required); the work is enqueued on `stream`
  * (NULL = legacy default stream) on the calling thread's current device.
- * Limits: at most 256 bodies and 2048 contacts, else PDC_EINVAL.  All calls share
- * the scratch and it keeps the last call's contents (the kernels reset what must
- * start at zero), so calls that overlap on the GPU race: serialise them.  The
- * first call on each device performs a one-time set-up (it looks up the scratch's
- * device address); make it before any stream capture.  out->stats is zeroed, not
- * filled.  Errors are reported through pdc_last_error(NULL). */
+ * Limits: at most 256 bodies and 2048 contacts, else PDC_EINVAL; the sparse
+ * factor's capacity (3,072 off-diagonal blocks) is the same as pdc_solve's, so a
+ * scene inside the limits takes the same branch and gets the same results as
+ * pdc_solve_async with warp teams off.  All calls share the scratch and it keeps
+ * the last call's contents (the kernels reset what must start at zero), so calls
+ * that overlap on the GPU race: serialise them.  Each call outside a stream
+ * capture looks up the scratch's device address for the current device (so a
+ * cudaDeviceReset between calls is harmless); a call made while `stream` is
+ * capturing reuses the address found by the last uncaptured call on that device,
+ * so make one call on each device before any capture.  `stats` (a DEVICE pointer
+ * to one pdc_stats, may be NULL) receives the solve's statistics and status;
+ * out->stats is zeroed, not filled.  Errors are reported through
+ * pdc_last_error(NULL). */
 int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
                       const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts,
-                      pdc_result* out, void* stream);
+                      pdc_result* out, pdc_stats* stats, void* stream);
 
 /* ------------------------------------------------------------------------
  * Device-resident time stepping (DynamicSystem::step, src/Dynamics/DynamicSystem.cpp:130-218,
@@ -346,6 +359,13 @@ const char* pdc_last_error(const pdc_solver* s);
 
 /* Library version string. */
 const char* pdc_version(void);
+
+/* Host-side fault injection, for tests of the failure paths (no counterpart in
+ * the reference): the next `n` device allocations made by this library (solver
+ * workspaces, world and server set-up) fail as if the device were out of memory,
+ * so the calls that need them return PDC_ENOMEM and leave their handles usable.
+ * n = 0 cancels.  Process-wide; not thread-safe against concurrent allocations. */
+void pdc_fault_inject_alloc(int32_t n);
 
 /* Page-locked host memory for the host-array calls (no counterpart in the
  * reference): inputs and outputs of pdc_solve / pdc_batch_solve placed in it are

@@ -988,7 +988,7 @@ static void fill_forces_intl(Problem& P, pdc_stats* st) {
             dl[2 * c + 1] = -P.invC[2 * c + 1] * (P.lambda[2 * c + 1] * (gr[0] * d[1] + gr[1] * d[2]) + rl[2 * c + 1]);
         }
 
-        LSResult ls = line_search(P, du, df, dl, sErr, sacErr, muc, 10);
+        LSResult ls = line_search(P, du, df, dl, sErr, sacErr, muc, P.cfg.ls_max_trials);  // 10 (:437-440)
         bool useGD = false;
         if (ls.step == 0) {  // gradient-descent fallback (:444-467)
             useGD = true;
@@ -996,7 +996,7 @@ static void fill_forces_intl(Problem& P, pdc_stats* st) {
             for (size_t q = 0; q < n_rigid; ++q) du[q] = -ru[q];
             df = rf;
             dl = rl;
-            ls = line_search(P, du, df, dl, sErr, sacErr, muc, 20);
+            ls = line_search(P, du, df, dl, sErr, sacErr, muc, P.cfg.gd_max_trials);  // 20 (:454-456)
             if (ls.step == 0) P.ls_fail = true;
         }
         P.vels = ls.u;

@@ -7,7 +7,7 @@ import ctypes as C
 
 import numpy as np
 
-PDC_ABI_VERSION = 2
+PDC_ABI_VERSION = 3
 
 PDC_OK, PDC_EINVAL, PDC_ECUDA, PDC_ENOMEM, PDC_ETIMEOUT, PDC_ENODEV, PDC_EBUSY = range(7)
 STATUS_NAMES = {0: "PDC_OK", 1: "PDC_EINVAL", 2: "PDC_ECUDA", 3: "PDC_ENOMEM",
@@ -61,6 +61,9 @@ class Config(C.Structure):
         ("mixed_inner_rtol", C.c_double),
         ("warm_start", C.c_int32),
         ("device", C.c_int32),
+        ("ls_max_trials", C.c_int32),
+        ("gd_max_trials", C.c_int32),
+        ("barrier_timeout_us", C.c_int64),
     ]
 
 
@@ -221,6 +224,9 @@ def default_config(**overrides):
     cfg.mixed_inner_rtol = 1e-3
     cfg.warm_start = 0
     cfg.device = 0
+    cfg.ls_max_trials = 10
+    cfg.gd_max_trials = 20
+    cfg.barrier_timeout_us = 10000000
     for k, v in overrides.items():
         setattr(cfg, k, v)
     return cfg

@@ -8,6 +8,7 @@
 #include <time.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -21,6 +22,8 @@
 namespace {
 
 thread_local std::string g_create_error;
+// pdc_fault_inject_alloc: device allocations still to fail
+std::atomic<int> g_fail_allocs{0};
 constexpr int kThreads = 256;
 constexpr int kWarpsPerBlock = kThreads / 32;
 // sparse scratch: bitsets, orders, offsets, 2x256 diagonal blocks, 3 node vectors
@@ -69,6 +72,28 @@ struct pdc_solver {
     int* d_counter = nullptr;
 };
 
+// Every device allocation of the library goes through here, so that tests can
+// make it fail on the host (pdc_fault_inject_alloc).
+static cudaError_t dev_malloc(void** p, size_t bytes) {
+    int left = g_fail_allocs.load();
+    while (left > 0) {
+        if (g_fail_allocs.compare_exchange_weak(left, left - 1)) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+template <typename T>
+static cudaError_t dev_malloc(T** p, size_t bytes) {
+    void* v = nullptr;
+    cudaError_t e = dev_malloc(&v, bytes);
+    *p = static_cast<T*>(v);
+    return e;
+}
+
+extern "C" void pdc_fault_inject_alloc(int32_t n) { g_fail_allocs.store(n > 0 ? n : 0); }
+
 static int fail(pdc_solver* s, int code, const std::string& msg) {
     if (s) s->err = msg;
     else g_create_error = msg;
@@ -114,6 +139,8 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
     e.max_direct = c.pcg_max_direct;
     e.rtol_iter = c.pcg_rtol_iter;
     e.max_cg = c.pcg_max_iter;
+    e.ls_max = c.ls_max_trials;
+    e.gd_max = c.gd_max_trials;
     return e;
 }
 
@@ -220,7 +247,7 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
         if (s->arena.base) cudaFree(s->arena.base);
         s->arena.base = nullptr;
         s->arena.cap = 0;
-        cudaError_t e = cudaMalloc(&s->arena.base, cap);
+        cudaError_t e = dev_malloc(&s->arena.base, cap);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return cuda_fail(s, e, "cudaMalloc(workspace)");
@@ -233,7 +260,7 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
         if (s->d_cost) cudaFree(s->d_cost);
         s->d_cost = nullptr;
         s->cost_cap = 0;
-        cudaError_t e = cudaMalloc(&s->d_cost, std::max(ns, 1) * sizeof(unsigned int));
+        cudaError_t e = dev_malloc(&s->d_cost, std::max(ns, 1) * sizeof(unsigned int));
         if (e != cudaSuccess) {
             cudaGetLastError();
             return cuda_fail(s, e, "cudaMalloc(scene costs)");
@@ -249,7 +276,7 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
     // sparse-factor slot of the large-scene teams, once a batch can hold a large scene
     if (!s->d_sparse_big && s->cfg.grid_min_bodies > 0 && nb >= s->cfg.grid_min_bodies &&
         s->cfg.sparse_max_bodies_large > 0) {
-        cudaError_t e = cudaMalloc(&s->d_sparse_big, kSparseBigDoubles * sizeof(double));
+        cudaError_t e = dev_malloc(&s->d_sparse_big, kSparseBigDoubles * sizeof(double));
         if (e != cudaSuccess) {
             cudaGetLastError();
             s->d_sparse_big = nullptr;
@@ -294,6 +321,9 @@ extern "C" void pdc_config_default(pdc_config* c) {
     c->mixed_inner_rtol = 1e-3;
     c->warm_start = 0;
     c->device = 0;
+    c->ls_max_trials = 10;  // PrimalDualForceSolver.cpp:437-440
+    c->gd_max_trials = 20;  // :454-456
+    c->barrier_timeout_us = 10000000;
 }
 
 static int validate_config(pdc_solver* s, const pdc_config* c) {
@@ -312,6 +342,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
         return fail(s, PDC_EINVAL, "sparse_max_bodies out of [0, 256]");
     if (c->sparse_max_bodies_large < 0 || c->sparse_max_bodies_large > pdc::kSparseMaxLarge)
         return fail(s, PDC_EINVAL, "sparse_max_bodies_large out of [0, 2048]");
+    if (c->ls_max_trials < 0 || c->gd_max_trials < 0) return fail(s, PDC_EINVAL, "negative line-search trials");
+    if (c->barrier_timeout_us <= 0) return fail(s, PDC_EINVAL, "barrier_timeout_us must be positive");
     return PDC_OK;
 }
 
@@ -338,8 +370,8 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         e = (s->threads == 128)
                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel<128>, 128, 0)
                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->blocks_per_sm, pdc::solve_scenes_kernel<256>, 256, 0);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_timers, 4 * sizeof(unsigned long long) + 16);
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_counter, 16);
+    if (e == cudaSuccess) e = dev_malloc(&s->d_timers, 4 * sizeof(unsigned long long) + 16);
+    if (e == cudaSuccess) e = dev_malloc(&s->d_counter, 16);
     if (e == cudaSuccess) e = cudaMemset(s->d_timers, 0, 4 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -353,7 +385,7 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pdc::solve_scene_grid_kernel<256>, 256, 0);
         s->grid_blocks = std::max(1, bps) * s->num_sms;
         const size_t bytes = 256 + 2 * (size_t)s->grid_blocks * 8 * sizeof(double) + (s->grid_blocks + 1) * sizeof(int);
-        if (e == cudaSuccess) e = cudaMalloc(&s->d_grid, bytes);
+        if (e == cudaSuccess) e = dev_malloc(&s->d_grid, bytes);
         if (e == cudaSuccess) e = cudaMemset(s->d_grid, 0, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -367,6 +399,7 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         s->gsync.err = reinterpret_cast<int*>(g + 128);
         s->gsync.partials = reinterpret_cast<double*>(g + 256);
         s->gsync.ipartials = reinterpret_cast<int*>(g + 256 + 2 * (size_t)s->grid_blocks * 8 * sizeof(double));
+        s->gsync.wait_ns = (unsigned long long)cfg->barrier_timeout_us * 1000ull;
     }
     // cluster team: the largest cluster (16, 8, 4 or 2 CTAs) the kernel can run
     cudaFuncSetAttribute(pdc::solve_scene_cluster_kernel<256>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -415,6 +448,22 @@ extern "C" int pdc_reset(pdc_solver* s) {
     s->newton_total = 0;
     s->solves = 0;
     return PDC_OK;
+}
+
+// After the device work is done: if a whole-GPU solve's grid barrier timed out,
+// clear the flag (so later launches run) and report PDC_ETIMEOUT; its scenes'
+// results are invalid.  `st` is the stream to read on (nullptr: synchronous).
+static int grid_error(pdc_solver* s, cudaStream_t st) {
+    int err = 0;
+    if (st) {
+        CK(cudaMemcpyAsync(&err, s->gsync.err, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H grid error");
+        CK(cudaStreamSynchronize(st), "sync");
+    } else {
+        CK(cudaMemcpy(&err, s->gsync.err, sizeof(int), cudaMemcpyDeviceToHost), "D2H grid error");
+    }
+    if (!err) return PDC_OK;
+    CK(cudaMemset(s->gsync.err, 0, sizeof(int)), "reset grid error");
+    return fail(s, PDC_ETIMEOUT, "grid barrier timed out in a whole-GPU scene solve");
 }
 
 // Enqueue the planner and the batched solve; then, one cooperative whole-GPU
@@ -700,7 +749,7 @@ extern "C" int pdc_sync(pdc_solver* s, int32_t timeout_ms) {
     long long waited = 0;
     for (;;) {
         cudaError_t e = cudaStreamQuery(s->stream);
-        if (e == cudaSuccess) return PDC_OK;
+        if (e == cudaSuccess) return grid_error(s, nullptr);
         if (e != cudaErrorNotReady) return cuda_fail(s, e, "stream");
         if (waited >= limit_us) return fail(s, PDC_ETIMEOUT, "pdc_sync timed out");
         struct timespec ts = {0, 50000};
@@ -761,20 +810,24 @@ extern "C" void pdc_host_free(void* p) {
 // output buffer (device pointers).
 //
 // Limits: at most kNoAllocMaxBodies bodies and kNoAllocMaxContacts contacts
-// per call; larger scenes are rejected with PDC_EINVAL.  Every GPU that loads
-// the library holds the 2 MiB array until the process exits.  All calls share
-// it and it keeps the last call's contents: the planner kernel resets the work
-// counters and each solve initialises every scratch value it reads, so nothing
-// needs clearing between calls -- but calls that overlap on the GPU (different
-// streams, threads or processes sharing the context) race on it.  The first
-// call on a device looks up the array's device address (cudaGetSymbolAddress,
-// once per device, with that device current); make that first call before any
-// stream capture.
+// per call; larger scenes are rejected with PDC_EINVAL.  The array holds the
+// solver arrays of a scene at those limits plus one full sparse-factor slot
+// (the same kSparseBlocks off-diagonal blocks a handle gives each team), so a
+// scene inside the limits takes the same branch as in pdc_solve.  Every GPU
+// that loads the library holds the 3 MiB array until the process exits.  All
+// calls share it and it keeps the last call's contents: the planner kernel
+// resets the work counters and each solve initialises every scratch value it
+// reads, so nothing needs clearing between calls -- but calls that overlap on
+// the GPU (different streams, threads or processes sharing the context) race
+// on it.  The array's device address is looked up (cudaGetSymbolAddress, with
+// the caller's device current) on every call whose stream is not capturing, so
+// it stays right after a cudaDeviceReset; a call on a capturing stream reuses
+// the address the last uncaptured call on that device found.
 namespace {
 constexpr int kNoAllocMaxBodies = 256;
 constexpr int kNoAllocMaxContacts = 2048;
-constexpr long long kNoAllocSparseDoubles = kSparseHeaderDoubles + 36LL * 1024;  // one team slot
-constexpr long long kNoAllocDoubles = 262144;                                     // 2 MiB
+constexpr long long kNoAllocSparseDoubles = kSparseHeaderDoubles + 36LL * kSparseBlocks;  // one team slot
+constexpr long long kNoAllocDoubles = 393216;                                              // 3 MiB
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
@@ -784,7 +837,7 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
                                  const pdc_bodies_soa* bodies, const pdc_contacts_soa* contacts, pdc_result* out,
-                                 void* stream) {
+                                 pdc_stats* stats, void* stream) {
     int rc = validate_config(nullptr, cfg);
     if (rc) return rc;
     if (!gravity || !bodies || !contacts || !out || !out->dvel || !out->dang_vel || !out->local_force)
@@ -803,10 +856,17 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
         return fail(nullptr, PDC_ENODEV, std::string("pdc_solve_noalloc: no device: ") + cudaGetErrorString(e));
     }
     if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: device ordinal");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, PDC_ECUDA, std::string("pdc_solve_noalloc: stream: ") + cudaGetErrorString(e));
+    }
     double* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {  // once per device, with that device current
+        if (cap == cudaStreamCaptureStatusNone) {  // with the caller's device current
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) {
@@ -818,6 +878,10 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
         }
         base = g_noalloc_ptr[dev];
     }
+    if (!base)
+        return fail(nullptr, PDC_EINVAL,
+                    "pdc_solve_noalloc: first call on this device made during a stream capture; call it once "
+                    "outside a capture first");
     // carve the workspace out of the fixed array: solver arrays, then one
     // sparse-factor slot (the scene runs on a single thread block, team slot 0)
     pdc::BatchPtrs P;
@@ -851,13 +915,12 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
     P.dvel = out->dvel;
     P.dang = out->dang_vel;
     P.lforce = out->local_force;
-    P.stats = nullptr;
+    P.stats = stats;
     P.timers = nullptr;
     std::memset(&out->stats, 0, sizeof(out->stats));
     pdc::EngineCfg C = engine_cfg(*cfg);
     C.warp_max_contacts = 0;  // one thread block: only team slot 0 of the sparse scratch is used
     C.warp_max_bodies = 0;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     pdc::plan_scenes_kernel<<<1, 1024, 0, st>>>(P, C);
     e = cudaGetLastError();
     if (e == cudaSuccess) {

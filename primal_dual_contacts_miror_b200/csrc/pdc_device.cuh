@@ -239,19 +239,19 @@ struct WarpTeam {
 };
 
 // Grid-wide team for one large scene: a cooperative launch (all blocks
-// co-resident), a sense-reversing grid barrier whose spin is bounded (on time-out
-// it raises `err`, after which every barrier returns at once so the kernel ends),
-// and reductions through per-block partials read back in a fixed block order
-// (double-buffered, so one barrier per reduction).
+// co-resident), a grid barrier whose wait is bounded (on time-out it raises
+// `err` and every block of the launch ends at that barrier), and reductions
+// through per-block partials read back in a fixed block order (double-buffered,
+// so one barrier per reduction).
 struct GridSync {
-    unsigned int* count;  // arrivals of the current generation
+    unsigned int* count;  // arrivals so far (zeroed before the launch)
     unsigned int* gen;    // generation counter
-    int* err;             // set on a barrier time-out
+    int* err;             // set on a barrier time-out; read and cleared by the host
     double* partials;     // [2][gridDim][8]
     int* ipartials;       // [gridDim + 1] block sums for scans
+    unsigned long long wait_ns;  // bound on one wait (pdc_config::barrier_timeout_us)
 };
 #define PDC_BARRIER_SPIN_LIMIT (1LL << 26)
-#define PDC_BARRIER_WAIT_NS 10000000000ULL  // 10 s
 
 struct GridTeam {
     static constexpr int kind = 2;
@@ -272,16 +272,21 @@ struct GridTeam {
     }
     // Grid barrier on a counter that only grows (zeroed before the launch): the
     // k-th barrier is passed once the counter reaches k * gridDim.x.  One
-    // release-atomic per block to arrive, acquire loads to wait; a wait longer
-    // than PDC_BARRIER_WAIT_NS sets the error flag, after which every barrier is
-    // skipped and the kernel runs out its bounded loops.
+    // release-atomic per block to arrive, acquire loads to wait.  A wait longer
+    // than G.wait_ns (or PDC_BARRIER_SPIN_LIMIT polls) sets the error flag; a
+    // block that sees the flag, its own or another's, ends right there (every
+    // thread exits), so no block reads data past a barrier that was not passed:
+    // the blocks still running are at most in the phase before it, on data of a
+    // barrier they did pass, and they stop at the next barrier.
     unsigned int epoch = 0;
     __device__ void sync() {
+        __shared__ int s_stop;
         __syncthreads();
         if (threadIdx.x == 0) {
             volatile int* err = G.err;
             ++epoch;
-            if (!*err) {
+            int stop = *err;
+            if (!stop) {
                 const unsigned int target = epoch * gridDim.x;
                 unsigned int v;
                 __threadfence();
@@ -291,14 +296,15 @@ struct GridTeam {
                 unsigned long long t0 = 0;
                 while ((int)(v - target) < 0) {
                     ++spins;
-                    if ((spins & 1023) == 1) {
+                    if ((spins & 63) == 1) {  // the clock every 64 polls
                         unsigned long long t;
                         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
                         if (spins == 1) t0 = t;
-                        else if (t - t0 > PDC_BARRIER_WAIT_NS) spins = PDC_BARRIER_SPIN_LIMIT + 1;
+                        else if (t - t0 > G.wait_ns) spins = PDC_BARRIER_SPIN_LIMIT + 1;
                     }
                     if (spins > PDC_BARRIER_SPIN_LIMIT || *err) {
                         atomicExch(G.err, 1);
+                        stop = 1;
                         break;
                     }
                     if (spins > 64) __nanosleep(20);
@@ -306,8 +312,10 @@ struct GridTeam {
                 }
                 __threadfence();
             }
+            s_stop = stop;
         }
         __syncthreads();
+        if (s_stop) asm volatile("exit;");
     }
     template <int N, bool MAX>
     __device__ __forceinline__ void reduce(double (&v)[N]) {

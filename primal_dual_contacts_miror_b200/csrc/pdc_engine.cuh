@@ -51,6 +51,8 @@ struct EngineCfg {
     int max_direct;
     double rtol_iter;
     int max_cg;
+    int ls_max;  // line-search trials of a Newton step (PrimalDualForceSolver.cpp:437-440)
+    int gd_max;  // ... and of the gradient-descent fallback (:454-456)
 };
 
 struct BatchPtrs {
@@ -819,6 +821,13 @@ class SceneSolver {
                 pcg_total += iters;
                 iters = conv ? 0 : maxit;  // the Hu rule sees a capped solve as maxCGIt
             } else {
+            // attempt 0: the solve; attempt 1 (iterative branch only): the
+            // reference's fallback when AMGCL ends non-finite, an Eigen CG from
+            // zero to machine precision with at most 2 n iterations (:416-421)
+            double rtol_a = rtol;
+            int maxit_a = maxit;
+            for (int attempt = 0; attempt < 2; ++attempt) {
+            iters = 0;
             if (!direct) {
                 // AMGCL starts from the previous du taken as the scaled unknown
                 // (:406-415), i.e. from D du here (this PCG runs on the unscaled
@@ -827,7 +836,8 @@ class SceneSolver {
                 for (int i = tid; i < n_local; i += nt) {
                     const int gb = B.lbody[b0 + i];
                     if (!active(gb)) continue;
-                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = bn > 0 ? B.dsc[6 * gb + r] * B.du[6 * gb + r] : 0.0;
+                    for (int r = 0; r < 6; ++r)
+                        B.du[6 * gb + r] = (bn > 0 && attempt == 0) ? B.dsc[6 * gb + r] * B.du[6 * gb + r] : 0.0;
                 }
                 T.sync();
                 spmv_to_X(B.du, nullptr, 0.0);
@@ -862,8 +872,8 @@ class SceneSolver {
             double beta = 0;
             if (bn == 0) {
                 // zero right-hand side: du = x0 (zero on the direct branch)
-            } else if (!(res < rtol)) {
-                for (iters = 0; iters < maxit;) {
+            } else if (!(res < rtol_a)) {
+                for (iters = 0; iters < maxit_a;) {
                     // p_new = z + beta p (p double-buffered by parity so that the
                     // neighbours' previous directions stay readable) and q = A p_new
                     const double* pp = (iters & 1) ? B.p2 : B.p;
@@ -915,13 +925,24 @@ class SceneSolver {
                     T.sum(s4);
                     ++iters;
                     res = sqrt(s4[0]) / bn;
-                    if (!(res >= rtol)) break;  // converged or non-finite
+                    if (!(res >= rtol_a)) break;  // converged or non-finite
                     beta = s4[1] / rz;
                     rz = s4[1];
                 }
             }
-            pcg_total += iters;
-            if (!isfinite(res)) lin_bad = true;
+            if (direct || attempt == 1 || isfinite(res)) {
+                pcg_total += iters;  // the rerun's count replaces the first attempt's, as in the reference
+                if (!isfinite(res)) {
+                    if (direct) lin_bad = true;  // the LDLT failure rule (:390-394)
+                    else nonfinite = true;       // du is the CG fallback's, whatever it is
+                }
+                break;
+            }
+            nonfinite = true;
+            rtol_a = 2.220446049250313e-16;  // Eigen's default tolerance: machine epsilon
+            maxit_a = 2 * n_rigid;           // ... and iteration cap: twice the unknowns
+            T.sync();
+            }  // attempts
             }  // PCG branch
             if (lin_bad) {  // LDLT failure analogue (:390-394): du = 0
                 nonfinite = true;
@@ -954,7 +975,7 @@ class SceneSolver {
 
             // line search (:437-440), gradient-descent fallback (:444-467)
             int trials = 0;
-            double step = line_search(sErr, sacErr, muc, 10, trials);
+            double step = line_search(sErr, sacErr, muc, C.ls_max, trials);
             ls_total += trials;
             bool useGD = false;
             if (step == 0) {
@@ -973,7 +994,7 @@ class SceneSolver {
                     B.dl[2 * gc + 1] = B.rl[2 * gc + 1];
                 }
                 T.sync();
-                step = line_search(sErr, sacErr, muc, 20, trials);
+                step = line_search(sErr, sacErr, muc, C.gd_max, trials);
                 ls_total += trials;
                 if (step == 0) ls_fail = true;
             }

@@ -139,7 +139,7 @@ extern "C" int pdc_server_create(const pdc_config* cfg, double dt, const double 
     };
     Arena A;
     const size_t need = carve_server(A);
-    cudaError_t e = cudaMalloc(&v->mem, need);
+    cudaError_t e = dev_malloc(&v->mem, need);
     if (e == cudaSuccess) {
         A.base = v->mem;
         carve_server(A);

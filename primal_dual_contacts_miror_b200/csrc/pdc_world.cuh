@@ -409,7 +409,7 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
         return a.off + 256;
     };
     const size_t need = carve_world(A);
-    cudaError_t e = cudaMalloc(&w->mem, need);
+    cudaError_t e = dev_malloc(&w->mem, need);
     if (e == cudaSuccess) {
         A.base = w->mem;
         carve_world(A);
@@ -494,7 +494,7 @@ extern "C" int pdc_world_create(const pdc_config* cfg, int32_t n_scenes, const i
             return a.off + 256;
         };
         const size_t lneed = carve_large(la);
-        cudaError_t le = cudaMalloc(&w->large_mem, lneed + n_scenes);
+        cudaError_t le = dev_malloc(&w->large_mem, lneed + n_scenes);
         if (le == cudaSuccess) {
             la.base = w->large_mem;
             carve_large(la);
@@ -647,7 +647,7 @@ extern "C" int pdc_world_sync(pdc_world* w, int32_t timeout_ms) {
         waited += 50;
     }
     CK(cudaDeviceSynchronize(), "world sync");
-    return PDC_OK;
+    return w->large.empty() ? PDC_OK : grid_error(s, nullptr);
 }
 
 extern "C" int pdc_world_state(pdc_world* w, double* pos, double* quat, double* vel, double* ang_vel) {

@@ -91,6 +91,8 @@ def load():
     lib.pdc_host_alloc.restype = C.c_int
     lib.pdc_host_free.argtypes = [vp]
     lib.pdc_host_free.restype = None
+    lib.pdc_fault_inject_alloc.argtypes = [C.c_int32]
+    lib.pdc_fault_inject_alloc.restype = None
     _lib = lib
     return lib
 
@@ -98,8 +100,14 @@ def load():
 EXPORTED_SYMBOLS = [
     "pdc_config_default", "pdc_create", "pdc_destroy", "pdc_reset", "pdc_solve", "pdc_solve_async",
     "pdc_batch_solve", "pdc_batch_solve_async", "pdc_sync", "pdc_timings", "pdc_last_error", "pdc_version",
-    "pdc_host_alloc", "pdc_host_free",
+    "pdc_host_alloc", "pdc_host_free", "pdc_fault_inject_alloc",
 ]
+
+
+def fault_inject_alloc(n):
+    """Make the library's next `n` device allocations fail as out-of-memory
+    (host-side fault injection for tests; 0 cancels)."""
+    load().pdc_fault_inject_alloc(int(n))
 
 
 def pinned_empty(shape, dtype=np.float64):

@@ -82,3 +82,16 @@ def test_scene_stats_sequence_reads_each_scene_on_access():
         v[3]
     st[1].newton_iters = 99  # read when accessed: the dict reflects the record now
     assert v[1]["newton_iters"] == 99
+
+
+def test_config_mirror_matches_library_defaults():
+    """pdc_config_default fills the C struct; every field read through the ctypes
+    mirror equals abi.default_config(): the two layouts agree field by field."""
+    L = lib.load()
+    c = abi.Config()
+    L.pdc_config_default(C.byref(c))
+    d = abi.default_config()
+    for name, _ in abi.Config._fields_:
+        assert getattr(c, name) == getattr(d, name), name
+    assert c.abi_version == abi.PDC_ABI_VERSION == 3
+    assert c.ls_max_trials == 10 and c.gd_max_trials == 20  # PrimalDualForceSolver.cpp:437-440, 454-456
