@@ -162,6 +162,8 @@ typedef struct pdc_stats {
     int32_t factor_blocks;  /* off-diagonal 6x6 blocks of the sparse factor (0: PCG) */
     int32_t team;           /* 0: solved by a thread block, 1: by one warp, 2: by the whole GPU,
                                3: by a thread-block cluster */
+    int32_t n_contacts;     /* contacts of the scene (the solve's N_c) */
+    int32_t reserved;       /* zero */
     double exit_err;        /* exitErr at exit (:302-307) */
     double kkt_stationarity;/* max(|ru|/6N_b, |rf|/3N_c) */
     double kkt_complementarity; /* max(|lambda.c|_inf, dual gap) */
@@ -314,6 +316,19 @@ int pdc_world_collide(pdc_world* w);
 int pdc_world_sync(pdc_world* w, int32_t timeout_ms);
 /* Copy body state out (any pointer may be NULL). */
 int pdc_world_state(pdc_world* w, double* pos, double* quat, double* vel, double* ang_vel);
+/* Enqueue host -> device copies of the body state on `stream` (NULL = legacy
+ * default stream), packed as in pdc_shapes_soa; any pointer may be NULL to keep
+ * that part.  The host arrays must stay valid until the stream reaches the
+ * copies (page-locked memory from pdc_host_alloc copies by DMA).  With
+ * pdc_world_step and pdc_world_get_state this drives the device world from
+ * host-owned state, the way the reference's DynamicSystem owns its objects. */
+int pdc_world_set_state(pdc_world* w, const double* pos, const double* quat, const double* vel,
+                        const double* ang_vel, void* stream);
+/* Enqueue device -> host copies of the body state and of the last step's
+ * per-scene statistics (n_scenes records) on `stream`; any pointer may be NULL.
+ * Read them after synchronizing the stream. */
+int pdc_world_get_state(pdc_world* w, double* pos, double* quat, double* vel, double* ang_vel,
+                        pdc_stats* stats, void* stream);
 /* Copy the last contact sets out, scene by scene, compacted: counts[n_scenes], then
  * per contact body[2] (scene-local), frame[9], arm[6], depth, pos[3], local_force[3]. */
 int pdc_world_contacts(pdc_world* w, int32_t* counts, int32_t* body, double* frame, double* arm,

@@ -1040,6 +1040,7 @@ extern "C" int pdc_oracle_solve(const pdc_config* cfg, double dt, const double g
     if (!cfg || !bodies || !contacts || !out || !gravity) return PDC_EINVAL;
     const int nb = bodies->n, nc = contacts->n;
     std::memset(&out->stats, 0, sizeof(out->stats));
+    out->stats.n_contacts = nc;
     for (int b = 0; b < nb; ++b)
         for (int r = 0; r < 3; ++r) {
             out->dvel[3 * b + r] = gravity[r] * dt;  // :85-88

@@ -100,6 +100,8 @@ class Stats(C.Structure):
         ("n_local_bodies", C.c_int32),
         ("factor_blocks", C.c_int32),
         ("team", C.c_int32),
+        ("n_contacts", C.c_int32),
+        ("reserved", C.c_int32),
         ("exit_err", C.c_double),
         ("kkt_stationarity", C.c_double),
         ("kkt_complementarity", C.c_double),

@@ -2450,6 +2450,8 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
     st.n_local_bodies = 0;
     st.factor_blocks = 0;
     st.team = Team::kind;
+    st.n_contacts = S.nc;
+    st.reserved = 0;
     st.exit_err = 0;
     st.kkt_stationarity = 0;
     st.kkt_complementarity = 0;

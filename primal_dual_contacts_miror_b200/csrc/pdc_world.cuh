@@ -663,6 +663,42 @@ extern "C" int pdc_world_state(pdc_world* w, double* pos, double* quat, double* 
     return PDC_OK;
 }
 
+// Enqueue host -> device copies of the body state on `stream` (any pointer may
+// be NULL to keep that part).  The host arrays must stay valid until the stream
+// reaches the copies; in page-locked memory (pdc_host_alloc) they run as DMA.
+extern "C" int pdc_world_set_state(pdc_world* w, const double* pos, const double* quat, const double* vel,
+                                   const double* ang_vel, void* stream) {
+    if (!w) return PDC_EINVAL;
+    pdc_solver* s = w->solver;
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nb = w->nb;
+    if (pos) CK(cudaMemcpyAsync(w->W.pos, pos, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D pos");
+    if (quat) CK(cudaMemcpyAsync(w->W.quat, quat, 4 * nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D quat");
+    if (vel) CK(cudaMemcpyAsync(w->W.vel, vel, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D vel");
+    if (ang_vel) CK(cudaMemcpyAsync(w->W.ang, ang_vel, 3 * nb * sizeof(double), cudaMemcpyHostToDevice, st), "H2D ang");
+    return PDC_OK;
+}
+
+// Enqueue device -> host copies of the body state and of the last step's
+// per-scene statistics on `stream` (any pointer may be NULL); the caller
+// synchronizes the stream before reading them.
+extern "C" int pdc_world_get_state(pdc_world* w, double* pos, double* quat, double* vel, double* ang_vel,
+                                   pdc_stats* stats, void* stream) {
+    if (!w) return PDC_EINVAL;
+    pdc_solver* s = w->solver;
+    CK(cudaSetDevice(s->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nb = w->nb;
+    if (pos) CK(cudaMemcpyAsync(pos, w->W.pos, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H pos");
+    if (quat) CK(cudaMemcpyAsync(quat, w->W.quat, 4 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H quat");
+    if (vel) CK(cudaMemcpyAsync(vel, w->W.vel, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H vel");
+    if (ang_vel) CK(cudaMemcpyAsync(ang_vel, w->W.ang, 3 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H ang");
+    if (stats)
+        CK(cudaMemcpyAsync(stats, w->stats, w->ns * sizeof(pdc_stats), cudaMemcpyDeviceToHost, st), "D2H stats");
+    return PDC_OK;
+}
+
 extern "C" int pdc_world_contacts(pdc_world* w, int32_t* counts, int32_t* body, double* frame, double* arm,
                                   double* depth, double* pos, double* local_force) {
     if (!w || !counts) return PDC_EINVAL;

@@ -276,6 +276,63 @@ class World:
         return counts, {"body": body[:n], "frame": frame[:n], "arm": arm[:n], "depth": depth[:n], "pos": pos[:n],
                         "local_force": lf[:n]}
 
+    def set_state(self, pos=None, quat=None, vel=None, ang_vel=None, stream=None):
+        """Enqueue host -> device copies of the body state (float64 arrays packed
+        as the shapes; None keeps that part).  The arrays must stay alive until
+        the stream reaches the copies: use page-locked ones (pinned_empty) and
+        synchronize before reusing them."""
+        dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.pdc_world_set_state(self.h, dp(pos), dp(quat), dp(vel), dp(ang_vel),
+                                                 C.c_void_p(stream or 0)))
+
+    def get_state_async(self, pos=None, quat=None, vel=None, ang_vel=None, stats=None, stream=None):
+        """Enqueue device -> host copies of the body state and of the last step's
+        per-scene statistics (`stats`: a ctypes array of abi.Stats, n_scenes
+        long); read them after synchronizing the stream."""
+        dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+        sp = None if stats is None else C.cast(stats, C.POINTER(abi.Stats))
+        self._check(self.lib.pdc_world_get_state(self.h, dp(pos), dp(quat), dp(vel), dp(ang_vel), sp,
+                                                 C.c_void_p(stream or 0)))
+
+    def _world_inertia(self, quat):
+        """World-frame inertia and inverse (packed xx,yy,zz,xy,xz,yz) of every
+        body at orientations `quat`, from the principal moments."""
+        x, y, z, w = quat[:, 0], quat[:, 1], quat[:, 2], quat[:, 3]
+        R = np.stack([
+            np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+            np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+            np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+        i0 = self.shapes.inertia0
+        iw = np.einsum("nij,nj,nkj->nik", R, i0, R)
+        iwi = np.einsum("nij,nj,nkj->nik", R, 1.0 / i0, R)
+        s6 = lambda m: np.stack([m[:, 0, 0], m[:, 1, 1], m[:, 2, 2], m[:, 0, 1], m[:, 0, 2], m[:, 1, 2]], -1)
+        return s6(iw), s6(iwi)
+
+    def host_batch(self):
+        """Every scene's next contact problem (contacts regenerated from the
+        current poses, body state with world-frame inertia, scene-local body
+        ids) as one HostBatch with each scene's dt and gravity: the input its
+        next step's solve gets, for Solver.batch_solve or any other solver of
+        the same interface."""
+        self.collide()
+        self.sync()
+        pos, quat, vel, ang = self.state()
+        counts, c = self.contacts()
+        iw, iwi = self._world_inertia(quat)
+        bo = self.shapes.body_offsets
+        co = np.zeros(len(counts) + 1, np.int64)
+        co[1:] = np.cumsum(counts)
+        sc = []
+        for k in range(self.shapes.n_scenes):
+            b0, b1, c0, c1 = int(bo[k]), int(bo[k + 1]), int(co[k]), int(co[k + 1])
+            sc.append(abi.HostScene(vel[b0:b1], ang[b0:b1], self.shapes.mass[b0:b1], iw[b0:b1], iwi[b0:b1],
+                                    self.shapes.is_static[b0:b1], c["body"][c0:c1], c["frame"][c0:c1],
+                                    c["arm"][c0:c1], c["depth"][c0:c1]))
+        hb = abi.HostBatch(sc, 0.0, (0.0, 0.0, 0.0))
+        hb.dt = np.ascontiguousarray(self.shapes.dt, dtype=np.float64)
+        hb.gravity = np.ascontiguousarray(self.shapes.gravity, dtype=np.float64).reshape(-1, 3)
+        return hb
+
     def host_scene(self, k=0):
         """Scene k as the contact problem its next step would solve: contacts
         regenerated from the current poses (collide), body state with world-frame
@@ -414,6 +471,10 @@ def _bind_world(lib):
     lib.pdc_world_contacts.restype = C.c_int
     lib.pdc_world_stats.argtypes = [vp, C.POINTER(abi.Stats), ip]
     lib.pdc_world_stats.restype = C.c_int
+    lib.pdc_world_set_state.argtypes = [vp, dp, dp, dp, dp, vp]
+    lib.pdc_world_set_state.restype = C.c_int
+    lib.pdc_world_get_state.argtypes = [vp, dp, dp, dp, dp, C.POINTER(abi.Stats), vp]
+    lib.pdc_world_get_state.restype = C.c_int
     lib.pdc_server_create.argtypes = [C.POINTER(abi.Config), C.c_double, dp, C.c_int32, C.c_int64, C.c_int32,
                                       C.POINTER(vp)]
     lib.pdc_server_create.restype = C.c_int

@@ -9,13 +9,18 @@ reference's keys, defaults and errors: `DynamicSystem::fillFromYAML`
 `FileLoader::loadFile` (src/IO/FileLoader.cpp:14-29).  One key the reference
 ignores selects the backend: `simulation.solver.backend: gpu | cpu_oracle`.
 
-`load_scene` reads the `scene:` section.  The reference builds its bodies from
-glTF files (`cubes: "x.glb"`, FileLoader.cpp:41-84) and fits primitives to the
-meshes; glTF import is not part of this library, so bodies are given inline:
-`boxes: [{half: [..], pos: [..], quat: [x, y, z, w]}]`, `spheres: [{radius,
-pos}]`, `planes: [{point, normal: "+z"}]`, with the reference's `static:` and
-`initialize:` (id, density, velocity, angular_velocity) keys applied to the
-bodies in that order (boxes, then spheres, then planes).
+`load_scene` reads the `scene:` section as `FileLoader::loadScene` does
+(FileLoader.cpp:42-111): `cubes:` and `spheres:` name glTF binary files (one
+file or a list, relative to the YAML file), every mesh node of which becomes a
+box or sphere fitted to the mesh (primitives.py); bodies are numbered file by
+file, in the reference's type order (meshes, convex, cubes, ellipsoids,
+spheres), node order within a file; then `static:` and `initialize:` (id,
+density, velocity, angular_velocity) apply by body number.  Mesh, convex and
+ellipsoid bodies are not supported (the solver's narrow phase handles boxes,
+spheres and planes).  Bodies can also be given inline, numbered after the glTF
+ones: `boxes: [{half, pos, quat: [x, y, z, w], density}]`, `spheres: [{radius,
+pos, density}]`, `planes: [{point, normal: "+z"}]` (inline boxes and spheres
+default to density 1000, glTF ones to the reference's 1).
 """
 import os
 
@@ -102,42 +107,72 @@ def frames_to_bake(baking_time, timestep):
             return n
 
 
-def load_scene(src):
+def _entries(node, key):
+    v = node.get(key)
+    if v is None:
+        return []
+    return v if isinstance(v, list) else [v]
+
+
+def _gltf_files(node, key, base):
+    return [os.path.join(base, n) for n in _entries(node, key) if isinstance(n, str)]
+
+
+def load_scene(src, base_dir=None):
     """Bodies of a scene file's `scene:` section as a shape-scene dict (the
-    input of abi.ShapeBatch)."""
+    input of abi.ShapeBatch).  `base_dir`: where glTF names are resolved (the
+    YAML file's directory when `src` is a path)."""
+    from . import glb, primitives
+
     root = _load(src)
+    if base_dir is None:
+        base_dir = os.path.dirname(os.path.abspath(src)) if isinstance(src, (str, os.PathLike)) else "."
     node = root.get("scene") or {}
-    for key in ("meshes", "convex", "cubes", "ellipsoids", "spheres"):
-        if isinstance(node.get(key), str):
-            raise ValueError(f"scene.{key}: '{node[key]}' is a glTF file; glTF import is not supported, "
-                             "describe the bodies inline (boxes / spheres / planes)")
-    rows = []  # (kind, spec)
-    for b in node.get("boxes") or []:
-        rows.append(("box", b))
-    for s in node.get("spheres") or []:
-        rows.append(("sphere", s))
-    for p in node.get("planes") or []:
-        rows.append(("plane", p))
-    init = {int(o["id"]): o for o in (node.get("initialize") or [])}
-    static = {int(i) for i in (node.get("static") or [])}
-    sb = scenes.ShapeSceneBuilder()
-    for idx, (kind, spec) in enumerate(rows):
-        o = init.get(idx, {})
-        dens = float(o.get("density", spec.get("density", DEFAULT_DENSITY)))
-        vel = tuple(float(v) for v in o.get("velocity", spec.get("velocity", (0, 0, 0))))
-        ang = tuple(float(v) for v in o.get("angular_velocity", spec.get("angular_velocity", (0, 0, 0))))
-        st = idx in static
-        if kind == "box":
-            sb.add_box(tuple(float(h) for h in spec["half"]), tuple(float(p) for p in spec["pos"]), dens,
-                       quat=tuple(float(q) for q in spec.get("quat", (0, 0, 0, 1))), vel=vel, ang=ang, static=st)
-        elif kind == "sphere":
-            sb.add_sphere(float(spec["radius"]), tuple(float(p) for p in spec["pos"]), dens, vel=vel, ang=ang,
-                          static=st)
-        else:
-            sb.add_plane(tuple(float(p) for p in spec.get("point", (0, 0, 0))), spec.get("normal", "+z"))
-    if not rows:
+    for key in ("meshes", "convex", "ellipsoids"):
+        if node.get(key) is not None:
+            raise ValueError(f"scene.{key}: {key} bodies are not supported (boxes, spheres and planes only)")
+    rows = []  # (type, size, pos, quat, density)
+    for kind, key in (("cube", "cubes"), ("sphere", "spheres")):  # FileLoader.cpp:46-75 order
+        for path in _gltf_files(node, key, base_dir):
+            for n in glb.read(path):
+                f = primitives.fit(kind, n["matrix"], n["positions"], n["triangles"])
+                rows.append((f["type"], f["size"], f["pos"], primitives.rot_to_quat(f["rot"]), 1.0))
+    for b in (node.get("boxes") or []):
+        rows.append((0, np.array(b["half"], float), np.array(b["pos"], float),
+                     np.array(b.get("quat", (0, 0, 0, 1)), float), float(b.get("density", DEFAULT_DENSITY))))
+    for sp in (x for x in _entries(node, "spheres") if isinstance(x, dict)):
+        rows.append((1, np.array([float(sp["radius"]), 0, 0]), np.array(sp["pos"], float),
+                     np.array((0.0, 0.0, 0.0, 1.0)), float(sp.get("density", DEFAULT_DENSITY))))
+    n_solid = len(rows)
+    planes = list(node.get("planes") or [])
+    if not rows and not planes:
         raise ValueError("scene: no bodies")
-    return sb.build()
+    init = {}
+    for o in (node.get("initialize") or []):
+        if "id" not in o:
+            raise ValueError("object_init: id is required")
+        init[int(o["id"])] = o
+    static = {int(i) for i in (node.get("static") or [])}
+    n_all = n_solid + len(planes)
+    # The reference indexes its object list without a bounds check here
+    # (DynamicSystem.h:147), so an id past the last body is undefined behaviour
+    # there (scenes/dynamic_slide/dynamic_slide.yaml initializes id 2 of 2
+    # bodies); such entries are skipped and listed in the result's "warnings".
+    warnings = [f"scene: {k} body id {i} out of range (0..{n_all - 1}), ignored"
+                for k, ids in (("static", static), ("initialize", init)) for i in sorted(ids) if not 0 <= i < n_all]
+    sb = scenes.ShapeSceneBuilder()
+    for idx, (t, size, pos, quat, dens) in enumerate(rows):
+        o = init.get(idx, {})
+        dens = float(o.get("density", dens))
+        vel = tuple(float(v) for v in o.get("velocity", (0, 0, 0)))
+        ang = tuple(float(v) for v in o.get("angular_velocity", (0, 0, 0)))
+        m, i0 = primitives.mass_properties(t, size, dens)
+        sb.add(t, tuple(size), tuple(pos), tuple(quat), vel, ang, m, tuple(i0), idx in static)
+    for p in planes:
+        sb.add_plane(tuple(float(x) for x in p.get("point", (0, 0, 0))), p.get("normal", "+z"))
+    out = sb.build()
+    out["warnings"] = warnings
+    return out
 
 
 def run(scene_file, output_file, frames=None):

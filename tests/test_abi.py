@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_sizes_match_header_layout():
     # the C structs are plain data; sizes pin the ctypes mirror to the header
-    assert C.sizeof(abi.Stats) == 8 * 4 + 6 * 8
+    assert C.sizeof(abi.Stats) == 10 * 4 + 6 * 8
     assert C.sizeof(abi.Bodies) == 8 + 6 * 8
     assert C.sizeof(abi.Contacts) == 8 + 5 * 8
 

@@ -17,17 +17,27 @@ def _free_port():
 
 
 def _rank_main(rank, world, port, q):
+    try:
+        _rank_body(rank, world, port, q)
+    except BaseException as e:  # report instead of leaving the parent waiting
+        q.put((rank, "error", repr(e), None, None))
+        raise
+
+
+def _rank_body(rank, world, port, q):
     import datetime
 
     import torch.distributed as dist
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     import bench
     import oracle_lib
-    from primal_dual_contacts_miror_b200 import abi
+    from primal_dual_contacts_miror_b200 import abi, scenes
 
-    batch = bench.build_workload(6, bench.rank_seed(rank))
+    # each rank's scenes come from its own seed (the bench's box drops on a GPU;
+    # settled piles here, which the oracle solves without one)
+    batch = abi.HostBatch(scenes.pile_batch(6, bench.rank_seed(rank)), bench.DT, bench.GRAVITY)
     dv, da, lf, st = oracle_lib.batch_solve(batch, cfg=abi.default_config(tol=1e-6))
     local_time = 0.5 + rank  # stand-in per-rank time
     tmax = bench.max_over_ranks(local_time, world, "cpu")
@@ -48,7 +58,8 @@ def test_two_ranks_shard_and_reduce_max():
     procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    res = sorted(q.get(timeout=600) for _ in range(2))
+    res = sorted(q.get(timeout=300) for _ in range(2))
+    assert all(r[1] != "error" for r in res), res
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0

@@ -91,6 +91,7 @@ def test_inline_scene_bodies():
     np.testing.assert_allclose(sc["quat"][2], [0, 0.0998334, 0, 0.9950042])
 
 
-def test_gltf_scene_is_rejected_clearly():
-    with pytest.raises(ValueError, match="glTF"):
-        yamlcfg.load_scene({"scene": {"cubes": "inverted_cubes.glb"}})
+def test_unsupported_body_kinds_are_rejected_clearly():
+    for key in ("meshes", "convex", "ellipsoids"):
+        with pytest.raises(ValueError, match="not supported"):
+            yamlcfg.load_scene({"scene": {key: "bunny.glb"}})
