@@ -1,5 +1,12 @@
 """Trajectory writer in the reference's output format (`FileSaver::saveToFile`,
-src/IO/FileSaver.cpp:137-206), for scenes stepped by the device world.
+src/IO/FileSaver.cpp:44-206), for scenes stepped by the device world.
+
+`<name>.gltf` (with its buffer in `<name>.bin`) is the scene (FileSaver.cpp:44-137):
+one mesh `mesh_<i>` per body, the body's collision geometry (a cube of
+half-extent 1 for boxes, an icosphere of radius 1 subdivided three times for
+spheres, a unit square for planes), and one top-level node per body with that
+mesh and the body's total transform at the last saved frame (rigid pose times
+the render scale), named by the body index.
 
 `<name>.npz` holds `time` (float64 [frames]) and, per body i, `mesh_<i>`
 (float64 [frames + 1, 7]): row 0 is the render scale of the body's collision
@@ -69,6 +76,102 @@ def render_scale(shape_type, size):
     return np.ones(3)
 
 
+def cube_mesh():
+    """Cube of half-extent 1: 24 vertices (4 per face, faces in -x, +x, -y, +y,
+    -z, +z order) and 12 outward triangles."""
+    pos, tri = [], []
+    for axis in range(3):
+        for sgn in (-1.0, 1.0):
+            a, b = [k for k in range(3) if k != axis]
+            base = len(pos)
+            for u, v in ((-1, -1), (1, -1), (1, 1), (-1, 1)):
+                p = [0.0, 0.0, 0.0]
+                p[axis], p[a], p[b] = sgn, u, v
+                pos.append(p)
+            n = np.zeros(3)
+            n[axis] = sgn
+            quad = [base, base + 1, base + 2, base + 3]
+            if np.dot(np.cross(np.subtract(pos[quad[1]], pos[quad[0]]), np.subtract(pos[quad[2]], pos[quad[0]])), n) < 0:
+                quad = quad[::-1]
+            tri += [[quad[0], quad[1], quad[2]], [quad[0], quad[2], quad[3]]]
+    return np.array(pos, np.float32), np.array(tri, np.uint32)
+
+
+def icosphere_mesh(subdivisions=3):
+    """Icosphere of radius 1: an icosahedron whose triangles are split in four
+    `subdivisions` times, new vertices pushed onto the sphere (642 vertices,
+    1,280 triangles at 3)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, float) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache, out = {}, []
+
+        def mid(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in cache:
+                m = verts[i] + verts[j]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            out += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = out
+    return np.array(verts, np.float32), np.array(faces, np.uint32)
+
+
+def square_mesh():
+    return (np.array([[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]], np.float32),
+            np.array([[0, 1, 2], [0, 2, 3]], np.uint32))
+
+
+def write_gltf(path, types, sizes, pos, quat):
+    """The scene file: per body a mesh of its collision geometry and a node with
+    the total transform [R diag(scale) | p]; buffers in `<base>.bin`."""
+    import json
+
+    base = os.path.splitext(path)[0]
+    meshes = {abi.PDC_SHAPE_BOX: cube_mesh(), abi.PDC_SHAPE_SPHERE: icosphere_mesh(3),
+              abi.PDC_SHAPE_PLANE: square_mesh()}
+    R = quat_to_matrix(np.asarray(quat, np.float64).reshape(-1, 4))
+    blob, views, accessors, gmeshes, nodes = bytearray(), [], [], [], []
+    for i, t in enumerate(types):
+        v, f = meshes[int(t)]
+        for arr, target, ctype, kind in ((v, 34962, 5126, "VEC3"), (f.reshape(-1), 34963, 5125, "SCALAR")):
+            raw = arr.astype(arr.dtype.newbyteorder("<")).tobytes()
+            views.append({"buffer": 0, "byteOffset": len(blob), "byteLength": len(raw), "target": target})
+            acc = {"bufferView": len(views) - 1, "componentType": ctype, "count": int(len(arr)), "type": kind}
+            if kind == "VEC3":
+                acc["min"] = [float(x) for x in v.min(0)]
+                acc["max"] = [float(x) for x in v.max(0)]
+            accessors.append(acc)
+            blob += raw + b"\0" * (-len(raw) % 4)
+        gmeshes.append({"name": f"mesh_{i}", "primitives": [
+            {"attributes": {"POSITION": len(accessors) - 2}, "indices": len(accessors) - 1, "mode": 4}]})
+        scale = render_scale(int(t), sizes[i])
+        if int(t) == abi.PDC_SHAPE_PLANE:
+            scale = np.full(3, 100.0)
+        M = np.eye(4)
+        M[:3, :3] = R[i] * scale[None, :]
+        M[:3, 3] = pos[i]
+        nodes.append({"name": str(i), "mesh": i, "matrix": [float(x) for x in M.T.reshape(-1)]})
+    doc = {"asset": {"version": "2.0", "generator": "primal_dual_contacts_miror_b200.filesaver"},
+           "buffers": [{"uri": os.path.basename(base) + ".bin", "byteLength": len(blob)}],
+           "bufferViews": views, "accessors": accessors, "meshes": gmeshes, "nodes": nodes,
+           "scenes": [{"name": "scene", "nodes": list(range(len(nodes)))}], "scene": 0}
+    with open(base + ".bin", "wb") as f:
+        f.write(bytes(blob))
+    with open(base + ".gltf", "w") as f:
+        json.dump(doc, f)
+    return base + ".gltf"
+
+
 class TrajectoryRecorder:
     """Collects the saved frames of one scene (`record` after each frame) and
     writes them in the reference's .npz/.info layout (`save`)."""
@@ -101,12 +204,16 @@ class TrajectoryRecorder:
         return out
 
     def save(self, path, info=""):
-        """Write `<path without extension>.npz` (stored, uncompressed entries) and
-        `<...>.info`; returns the two file names."""
+        """Write `<path without extension>.npz` (stored, uncompressed entries),
+        `<...>.info` and, once a frame was recorded, the scene `<...>.gltf` (+
+        `.bin`) at the last frame's poses; returns the .npz and .info names."""
         base = os.path.splitext(path)[0]
         np.savez(base + ".npz", **self.arrays())
         with open(base + ".info", "w") as f:
             f.write(info)
+        if self.frames:
+            last = self.frames[-1]
+            write_gltf(base + ".gltf", self.types, self.sizes, last[:, :3], last[:, 3:])
         return base + ".npz", base + ".info"
 
 
