@@ -163,7 +163,8 @@ typedef struct pdc_stats {
     int32_t team;           /* 0: solved by a thread block, 1: by one warp, 2: by the whole GPU,
                                3: by a thread-block cluster */
     int32_t n_contacts;     /* contacts of the scene (the solve's N_c) */
-    int32_t reserved;       /* zero */
+    int32_t precision_fallbacks; /* mixed precision: FP32 inner solves that broke down or stopped
+                               converging and were redone in FP64 */
     double exit_err;        /* exitErr at exit (:302-307) */
     double kkt_stationarity;/* max(|ru|/6N_b, |rf|/3N_c) */
     double kkt_complementarity; /* max(|lambda.c|_inf, dual gap) */

@@ -101,7 +101,7 @@ class Stats(C.Structure):
         ("factor_blocks", C.c_int32),
         ("team", C.c_int32),
         ("n_contacts", C.c_int32),
-        ("reserved", C.c_int32),
+        ("precision_fallbacks", C.c_int32),
         ("exit_err", C.c_double),
         ("kkt_stationarity", C.c_double),
         ("kkt_complementarity", C.c_double),

@@ -190,6 +190,9 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->dsc = D(6 * nb);
     P->inc = I(2 * nc);
     P->inc_o = I(2 * nc);
+    P->islot = I(2 * nc);
+    P->Xi = D(6 * nc);
+    P->armI = D(6 * nc);
     P->f = D(3 * nc);
     P->lam = D(2 * nc);
     P->fT = D(3 * nc);

@@ -109,6 +109,9 @@ struct BatchPtrs {
     // per-contact workspace
     int* inc;       // 2 per contact
     int* inc_o;     // 2 per contact: the incidence's other body (global index), -1 if static
+    int* islot;     // 2 per contact: incidence index of (contact, side), -1 for a static side
+    double* Xi;     // 3 per incidence: sigma X of its contact (sigma = -1 on side 0, +1 on side 1)
+    double* armI;   // 3 per incidence: the lever arm of its side
     double* f;      // 3
     double* lam;    // 2
     double* fT;     // 3
@@ -291,21 +294,30 @@ class SceneSolver {
         return C.mu;
     }
 
-    // Gather sum over the incidences of body gb of sigma * [X; c x X]
+    // Gather sum over the incidences of body gb of sigma * [X; c x X]: the
+    // contacts left sigma X in the body's own incidence slots (put_x), so the
+    // loads are contiguous and independent of each other
     __device__ __forceinline__ void gather(int gb, double out[6]) const {
         const int st = B.inc_start[gb], n = B.inc_cnt[gb];
+        const double* xi = B.Xi + 3LL * st;
+        const double* ai = B.armI + 3LL * st;
         double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+#pragma unroll 4
         for (int k = 0; k < n; ++k) {
-            const int e = B.inc[st + k];
-            const int gc = e >> 1, side = e & 1;
-            d3 x = ld3(B.X + 3 * gc);
-            d3 arm = ld3(B.arm + 6 * gc + 3 * side);
-            if (!side) x = scl3(-1.0, x);
-            d3 t = cross3(arm, x);
+            const d3 x = ld3(xi + 3 * k);
+            const d3 arm = ld3(ai + 3 * k);
+            const d3 t = cross3(arm, x);
             a0 += x.x; a1 += x.y; a2 += x.z;
             a3 += t.x; a4 += t.y; a5 += t.z;
         }
         out[0] = a0; out[1] = a1; out[2] = a2; out[3] = a3; out[4] = a4; out[5] = a5;
+    }
+    // Contact gc's world vector X into the incidence slots of its two sides, with
+    // the side's sign (-X for side 0, X for side 1; static sides have no slot)
+    __device__ __forceinline__ void put_x(int gc, d3 x) const {
+        const int s0 = B.islot[2 * gc], s1 = B.islot[2 * gc + 1];
+        if (s0 >= 0) st3(B.Xi + 3LL * s0, scl3(-1.0, x));
+        if (s1 >= 0) st3(B.Xi + 3LL * s1, x);
     }
     // (M / charMass) v  for an active body
     __device__ __forceinline__ void mass_mul(int gb, const double* v, double* y) const {
@@ -364,7 +376,10 @@ class SceneSolver {
             const int gc = c0 + c;
             for (int j = 0; j < 2; ++j) {
                 const int gb = b0 + B.cbody[2 * gc + j];
-                if (B.is_static[gb]) continue;
+                if (B.is_static[gb]) {
+                    B.islot[2 * gc + j] = -1;
+                    continue;
+                }
                 const int slot = atomicAdd(&B.inc_cur[gb], 1);
                 B.inc[B.inc_start[gb] + slot] = (gc << 1) | j;
             }
@@ -424,6 +439,8 @@ class SceneSolver {
                 spd = dmax(spd, B.X[3 * (e >> 1) + (e & 1)]);
                 const int go = b0 + B.cbody[2 * (e >> 1) + 1 - (e & 1)];
                 B.inc_o[st + k] = B.is_static[go] ? -1 : go;
+                B.islot[e] = st + k;  // e = 2 gc + side
+                st3(B.armI + 3LL * (st + k), ld3(B.arm + 6 * (e >> 1) + 3 * (e & 1)));
             }
             const double m = B.mass[gb];
             const double* I = B.inertia + 6 * gb;
@@ -446,7 +463,7 @@ class SceneSolver {
         {
             const int dmax = kLargeTeam ? C.dense_max_large : C.dense_max;
             const bool ws = kLargeTeam ? B.sparse_big != nullptr : B.dense != nullptr;
-            dense_mode = !C.mixed && ws && n_local < C.direct_threshold && dmax > 0 && n_active <= dmax &&
+            dense_mode = ws && n_local < C.direct_threshold && dmax > 0 && n_active <= dmax &&
                          n_active > 0 && dmax <= kSpMax;
         }
         if (dense_mode) {
@@ -569,53 +586,51 @@ class SceneSolver {
         ac2 += a0 * a0;
         if (rfo) { rfo[0] = r0; rfo[1] = 0; rfo[2] = 0; }
         if (rlo) { rlo[0] = rl0; rlo[1] = 0; }
-        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, 0.0, 0.0})));
+        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, 0.0, 0.0})));
     }
 
-    // Residual terms of one contact at state (uvec, f, lam) (nonSmoothResiduals :119-172,
-    // ACVector :53-73).  Writes X = -R f for the ru gather; returns squared norms.
-    __device__ __forceinline__ void contact_residual(int gc, const double* uvec, const double* fv, const double* lv,
-                                                     bool stored, double muc, double* rf_out, double* rl_out,
-                                                     double& wrf2, double& rl2, double& ac2) const {
+    // Residuals of one contact at the current iterate with its constraint values
+    // and gradient just computed (nonSmoothResiduals :119-172, ACVector :53-73),
+    // before the centering term is known: adds |wrf|^2, (lambda . c)^2 per
+    // constraint and |AC|^2; writes rf and X = -R f.
+    __device__ __forceinline__ void contact_residual_c(int gc, const double* uvec, const double* fv, double l0,
+                                                       double l1, double cn, double cc, double g0, double g1,
+                                                       double* rf_out, double& wrf2, double& a2, double& ac2) const {
         const Frame R = ld_frame(B.frame + 9 * gc);
         const d3 w = rel_vel(gc, uvec);
         st3(B.wu + 3 * gc, w);  // the line search steps from here: J(u + a du) = J u + a J du
+        const double fn = fv[0];
         if (C.only_normal) {
-            normal_residual(gc, R, w, fv[0], lv[0], muc, rf_out, rl_out, wrf2, rl2, ac2);
+            double rl2 = 0;
+            normal_residual(gc, R, w, fn, l0, 0.0, rf_out, nullptr, wrf2, rl2, ac2);
+            a2 += rl2;
             return;
         }
-        const double fn = fv[0], f1 = fv[1], f2 = fv[2];
+        const double f1 = fv[1], f2 = fv[2];
         const double mu = cmu(gc);
-        double g0, g1;
-        if (stored) { g0 = B.gr[2 * gc]; g1 = B.gr[2 * gc + 1]; }
-        else cone_grad(f1, f2, g0, g1);
         double r0 = 0 - w.x, r1 = 0 - w.y, r2 = 0 - w.z;
         if (C.spring_based) r0 -= compliance * cm * fn;
-        r0 += lv[0];
-        r1 -= lv[1] * g0;
-        r2 -= lv[1] * g1;
+        r0 += l0;
+        r1 -= l1 * g0;
+        r2 -= l1 * g1;
         r0 -= B.kn[gc];
-        double cn, cc;
-        if (stored) { cn = B.cv[2 * gc]; cc = B.cv[2 * gc + 1]; }
-        else { cn = -fn; cc = cone_c(fn, f1, f2, mu); }
-        const double rl0 = lv[0] * cn + muc, rl1 = lv[1] * cc + muc;
+        const double a0 = l0 * cn, a1 = l1 * cc;
         const double wt = tangential_weight(gc, R, w, fn);
         const double w1 = r1 * wt, w2 = r2 * wt;
         wrf2 += r0 * r0 + w1 * w1 + w2 * w2;
-        rl2 += rl0 * rl0 + rl1 * rl1;
+        a2 += a0 * a0 + a1 * a1;
         // Alart-Curnier (:60-70)
         const double tp = fn - (w.x + B.kn[gc] + spring_term * fn);
-        const double a0 = dmax(tp, 0.0) - fn;
+        const double q0 = dmax(tp, 0.0) - fn;
         const double rad = cone_radius(fn, mu);
         const double td0 = f1 - w.y, td1 = f2 - w.z;
         const double tdn = sqrt(td0 * td0 + td1 * td1);
         double p0 = td0, p1 = td1;
         if (!(tdn < rad)) { p0 = td0 * rad / tdn; p1 = td1 * rad / tdn; }
-        const double a1 = p0 - f1, a2 = p1 - f2;
-        ac2 += a0 * a0 + a1 * a1 + a2 * a2;
-        if (rf_out) { rf_out[0] = r0; rf_out[1] = r1; rf_out[2] = r2; }
-        if (rl_out) { rl_out[0] = rl0; rl_out[1] = rl1; }
-        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
+        const double q1 = p0 - f1, q2 = p1 - f2;
+        ac2 += q0 * q0 + q1 * q1 + q2 * q2;
+        rf_out[0] = r0; rf_out[1] = r1; rf_out[2] = r2;
+        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
     }
 
     // ru = M(u - uold) (+ gather of T_j f); static rows zero (calculateResiduals :151-163)
@@ -638,12 +653,17 @@ class SceneSolver {
         const bool direct = n_local < C.direct_threshold;
         double Hu = 1e-4, exitErr = 0;
         const double power = 0.66667;
-        int it = 0, pcg_total = 0, ls_total = 0, gd_total = 0;
+        int it = 0, pcg_total = 0, ls_total = 0, gd_total = 0, precision_fallbacks = 0;
         bool ls_fail = false, nonfinite = false;
         for (it = 0; it < C.max_iter; ++it) {
             t_mark = now();
-            // calculateConstraints (:105-118) + surrogateDualGap
-            double acc[1] = {0};  // lambda . c
+            // calculateConstraints (:105-118), surrogateDualGap and the residuals
+            // (:292-300) in one contact pass: the centering mu_c = 0.1 * gap is
+            // only known after the pass, so the pass keeps a = lambda . c per
+            // constraint and its sums, and |rl|^2 = sum (a + mu_c)^2 is expanded
+            // as sum a^2 + 2 mu_c sum a + n_cons mu_c^2 after the reduction; rl
+            // itself (= lambda c + mu_c) is formed where it is used
+            double e[5] = {0, 0, 0, 0, 0};  // ru2, wrf2, sum a^2, ac2, sum a
             for (int c = tid; c < nc; c += nt) {
                 const int gc = c0 + c;
                 const double fn = B.f[3 * gc], f1 = B.f[3 * gc + 1], f2 = B.f[3 * gc + 2];
@@ -661,17 +681,9 @@ class SceneSolver {
                 B.hs[3 * gc] = h0;
                 B.hs[3 * gc + 1] = h1;
                 B.hs[3 * gc + 2] = h2;
-                acc[0] += B.lam[2 * gc] * cn + B.lam[2 * gc + 1] * cc;
-            }
-            T.sum(acc);
-            const double sDualGap = -(acc[0] / n_cons);
-            const double muc = sDualGap * 0.1;
-            // residuals at the current iterate (:292-300)
-            double e[4] = {0, 0, 0, 0};  // ru2, wrf2, rl2, ac2
-            for (int c = tid; c < nc; c += nt) {
-                const int gc = c0 + c;
-                contact_residual(gc, B.u, B.f + 3 * gc, B.lam + 2 * gc, true, muc, B.rf + 3 * gc, B.rl + 2 * gc,
-                                 e[1], e[2], e[3]);
+                const double l0 = B.lam[2 * gc], l1 = B.lam[2 * gc + 1];
+                e[4] += l0 * cn + l1 * cc;
+                contact_residual_c(gc, B.u, B.f + 3 * gc, l0, l1, cn, cc, g0, g1, B.rf + 3 * gc, e[1], e[2], e[3]);
             }
             T.sync();
             for (int i = tid; i < n_local; i += nt) {
@@ -684,6 +696,9 @@ class SceneSolver {
                 body_residual(gb, B.u + 6 * gb, B.ru + 6 * gb, e[0]);
             }
             T.sum(e);
+            const double sDualGap = -(e[4] / n_cons);
+            const double muc = sDualGap * 0.1;
+            e[2] = e[2] + 2.0 * muc * e[4] + (double)n_cons * muc * muc;
             const double err = e[0] + e[1] + e[2];
             const double sErr = err, sacErr = e[0] + e[3] + e[2];
             const double eps = Hu * pow(err, power * 0.5);
@@ -706,7 +721,12 @@ class SceneSolver {
                 const double g0 = B.gr[2 * gc], g1 = B.gr[2 * gc + 1];
                 double lNorm = -ln * ic0;
                 if (C.spring_based) lNorm += compliance * cm;
-                const double rl0 = B.rl[2 * gc], rl1 = B.rl[2 * gc + 1];
+                // rl = lambda c + mu_c (nonSmoothResiduals :150-170), kept for the
+                // force recovery and the gradient-descent fallback
+                const double rl0 = ln * B.cv[2 * gc] + muc;
+                const double rl1 = C.only_normal ? 0.0 : lt * B.cv[2 * gc + 1] + muc;
+                B.rl[2 * gc] = rl0;
+                B.rl[2 * gc + 1] = rl1;
                 const double a = -lt * ic1;
                 const double sf0 = B.rf[3 * gc] + (-rl0 * ic0);
                 const double sf1 = B.rf[3 * gc + 1] + g0 * rl1 * ic1;
@@ -730,7 +750,7 @@ class SceneSolver {
                 if (C.mixed)
                     for (int q = 0; q < 6; ++q) B.Wf[6 * gc + q] = (float)B.W[6 * gc + q];
                 const d3 ks = d3{sf0 * kni, t00 * sf1 + t01 * sf2, t01 * sf1 + t11 * sf2};
-                st3(B.X + 3 * gc, from_frame(R, ks));
+                put_x(gc, from_frame(R, ks));
             }
             T.sync();
             // rhs = sum getTrans(j) K^-1 sf - ru; block-Jacobi blocks; PCG start
@@ -815,12 +835,27 @@ class SceneSolver {
             bool lin_bad = false;
             if (dense_mode) {
                 lin_bad = !dense_solve();
-            } else if (C.mixed) {
+            }
+            // mixed precision: FP32 PCG with FP64 refinement where PCG runs; an
+            // inner breakdown or a refinement that stops converging falls back
+            // to the FP64 PCG below, from zero
+            bool fp64_pcg = !dense_mode;
+            if (!dense_mode && C.mixed) {
                 bool conv = true;
-                lin_bad = !mixed_solve(eps, bnorm, rtol, iters, conv);
+                const bool ok = mixed_solve(eps, bnorm, rtol, iters, conv);
                 pcg_total += iters;
-                iters = conv ? 0 : maxit;  // the Hu rule sees a capped solve as maxCGIt
-            } else {
+                iters = 0;
+                fp64_pcg = !(ok && conv);
+                if (fp64_pcg) {
+                    ++precision_fallbacks;
+                    for (int i = tid; i < n_local; i += nt) {
+                        const int gb = B.lbody[b0 + i];
+                        for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = 0;
+                    }
+                    T.sync();
+                }
+            }
+            if (fp64_pcg) {
             // attempt 0: the solve; attempt 1 (iterative branch only): the
             // reference's fallback when AMGCL ends non-finite, an Eigen CG from
             // zero to machine precision with at most 2 n iterations (:416-421)
@@ -1014,6 +1049,7 @@ class SceneSolver {
         st.pcg_iters = pcg_total;
         st.ls_trials = ls_total;
         st.gd_fallbacks = gd_total;
+        st.precision_fallbacks = precision_fallbacks;
         int stt = status;
         if (it >= C.max_iter) stt |= PDC_SCENE_MAX_ITER;
         if (ls_fail) stt |= PDC_SCENE_LS_FAIL;
@@ -1930,7 +1966,10 @@ class SceneSolver {
                     s3[0] += (double)acc;
                 }
                 T.sum(s3);
+                // breakdown (p^T A p not positive in FP32, or a non-finite step):
+                // keep the correction so far, the FP64 residual decides
                 const float alpha = rz / (float)s3[0];
+                if (!(s3[0] > 0.0) || !isfinite(alpha)) break;
                 double s4[2] = {0, 0};
                 for (int i = tid; i < n_local; i += nt) {
                     const int gb = B.lbody[b0 + i];
@@ -1979,8 +2018,15 @@ class SceneSolver {
                 }
             }
             T.sum(s5);
+            const double prev = res;
             res = sqrt(s5[0]) / bnorm;
             if (!isfinite(res)) return false;
+            // a refinement step that does not halve the residual means the FP32
+            // solve cannot resolve this system: let the FP64 solve take it
+            if (outer > 0 && !(res < 0.5 * prev) && !(res < rtol)) {
+                conv = false;
+                break;
+            }
         }
         return true;
     }
@@ -2057,7 +2103,7 @@ class SceneSolver {
                 }
                 pv[j] = point_vel(pn, ld3(B.arm + 6 * gc + 3 * j));
             }
-            st3(B.X + 3 * gc, sym_mul(B.W + 6 * gc, sub3(pv[1], pv[0])));
+            put_x(gc, sym_mul(B.W + 6 * gc, sub3(pv[1], pv[0])));
         }
     }
     // (M/cm + eps I) x + gather(X)  for one active body
@@ -2330,7 +2376,7 @@ class SceneSolver {
         ac2 += a0 * a0 + a1 * a1 + a2 * a2;
         rfo[0] = r0; rfo[1] = r1; rfo[2] = r2;
         rlo[0] = rl0; rlo[1] = rl1;
-        st3(B.X + 3 * gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
+        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
     }
 
     // KKT report at the final iterate (mu_c = 0) and write-back (:491-510).
@@ -2451,7 +2497,7 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
     st.factor_blocks = 0;
     st.team = Team::kind;
     st.n_contacts = S.nc;
-    st.reserved = 0;
+    st.precision_fallbacks = 0;
     st.exit_err = 0;
     st.kkt_stationarity = 0;
     st.kkt_complementarity = 0;
