@@ -97,13 +97,16 @@ typedef struct pdc_config {
     int32_t precision;        /* enum pdc_precision */
     int32_t direct_threshold; /* local bodies below this use the direct-solve branch (2000) */
     int32_t sparse_max_bodies; /* direct branch: sparse block Cholesky on the device up to
-                                  this many active bodies (256, the maximum); larger
+                                  this many active bodies (256, the maximum; a batch of
+                                  many scenes holds one 9.7 MB factor slot per thread
+                                  block in flight, enough for any factor); larger
                                   scenes use PCG */
     int32_t sparse_max_bodies_large; /* the same for scenes solved by a thread-block cluster
                                   or the whole GPU (2048, the maximum; 0 = PCG) */
     int32_t warp_max_contacts; /* batched launch: scenes with at most this many contacts */
     int32_t warp_max_bodies;   /* and bodies are solved by one warp, larger ones by a
-                                  whole thread block (0 / 0 = blocks only, the default) */
+                                  whole thread block (0 / 0 = blocks only, the default;
+                                  at most 64 bodies when warp teams are on) */
     int32_t cta_threads;       /* threads per block of the solve kernel: 128 or 256 (256) */
     int32_t grid_min_bodies;   /* scenes with at least this many bodies are large: solved one
                                   launch each, by a thread-block cluster or the whole GPU
@@ -244,12 +247,12 @@ int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
  * captured), an engine that owns all device memory through its own pool or
  * budget, or a real-time loop that cannot afford an allocation's latency or
  * failure.  It needs no handle and calls no cudaMalloc/cudaFree: its scratch is
- * a fixed 3 MiB array inside the library (every GPU that loads the library holds
+ * a fixed 12 MiB array inside the library (every GPU that loads the library holds
  * it until exit).  Every pointer in bodies/contacts/out is a DEVICE pointer the
  * caller owns (is_static and depth required); the work is enqueued on `stream`
  * (NULL = legacy default stream) on the calling thread's current device.
  * Limits: at most 256 bodies and 2048 contacts, else PDC_EINVAL; the sparse
- * factor's capacity (3,072 off-diagonal blocks) is the same as pdc_solve's, so a
+ * factor's capacity (every pair of 256 bodies, 32,640 off-diagonal blocks) is the same as pdc_solve's, so a
  * scene inside the limits takes the same branch and gets the same results as
  * pdc_solve_async with warp teams off.  All calls share the scratch and it keeps
  * the last call's contents (the kernels reset what must start at zero), so calls

@@ -26,9 +26,14 @@ thread_local std::string g_create_error;
 std::atomic<int> g_fail_allocs{0};
 constexpr int kThreads = 256;
 constexpr int kWarpsPerBlock = kThreads / 32;
-// sparse scratch: bitsets, orders, offsets, 2x256 diagonal blocks, 3 node vectors
-constexpr long long kSparseHeaderDoubles = 30720;
-constexpr long long kSparseBlocks = 3072;  // off-diagonal L blocks per scene
+// sparse scratch of a thread-block team: bitsets, orders, offsets, 2x256
+// diagonal blocks, 4 node vectors, then room for any factor of 256 nodes
+constexpr long long kSparseHeaderDoubles = (pdc::kSparseHeaderBytes + 255) / 256 * 32;
+constexpr long long kSparseBlocks = pdc::kRowCap;  // off-diagonal L blocks per scene
+// a warp team's slot: the same fixed part, room for kWarpSparseBlocks blocks
+// (warp teams take scenes of at most kWarpMaxBodies bodies)
+constexpr int kWarpMaxBodies = 64;
+constexpr long long kWarpSparseBlocks = kWarpMaxBodies * (kWarpMaxBodies - 1) / 2;
 // large-scene teams: index arrays, node blocks and kRowCapLarge off-diagonal blocks
 constexpr long long kSparseBigDoubles = pdc::kSparseLargeHeaderDoubles + 36LL * pdc::kRowCapLarge;
 
@@ -146,7 +151,7 @@ static pdc::EngineCfg engine_cfg(const pdc_config& c) {
 
 // Workspace layout for a batch with totals (ns, nb, nc).
 static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs* P, bool host_inputs, int grid,
-                    int dense_max) {
+                    int dense_max, bool warp_teams) {
     A.reset();
     auto D = [&](size_t n) { return A.take<double>(n); };
     auto I = [&](size_t n) { return A.take<int>(n); };
@@ -226,13 +231,19 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->order_cta = I(ns);
     P->order_warp = I(ns);
     P->counts = I(4);
+    P->dense = nullptr;
+    P->dense_stride = 0;
+    P->dense_warp = nullptr;
+    P->dense_stride_warp = 0;
     if (dense_max > 0) {
-        // sparse factorisation scratch per team: fixed header + L blocks
+        // sparse factorisation scratch: one slot per thread block, and one per
+        // warp when warp teams are on
         P->dense_stride = kSparseHeaderDoubles + 36LL * kSparseBlocks;
-        P->dense = D((size_t)grid * (1 + kWarpsPerBlock) * P->dense_stride);
-    } else {
-        P->dense = nullptr;
-        P->dense_stride = 0;
+        P->dense = D((size_t)grid * P->dense_stride);
+        if (warp_teams) {
+            P->dense_stride_warp = kSparseHeaderDoubles + 36LL * kWarpSparseBlocks;
+            P->dense_warp = D((size_t)grid * kWarpsPerBlock * P->dense_stride_warp);
+        }
     }
     return A.off + 256;
 }
@@ -244,7 +255,8 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
     const int dmax = s->cfg.sparse_max_bodies;
     Arena probe;
     probe.base = nullptr;
-    size_t need = carve(probe, ns, nb, nc, P, host_inputs, grid, dmax);
+    const bool warp_teams = s->cfg.warp_max_contacts > 0 && s->cfg.warp_max_bodies > 0;
+    size_t need = carve(probe, ns, nb, nc, P, host_inputs, grid, dmax, warp_teams);
     if (need > s->arena.cap) {
         const size_t cap = std::max(need, s->arena.cap * 2);
         if (s->arena.base) cudaFree(s->arena.base);
@@ -257,7 +269,7 @@ static int ensure_arena(pdc_solver* s, int ns, long long nb, long long nc, pdc::
         }
         s->arena.cap = cap;
     }
-    carve(s->arena, ns, nb, nc, P, host_inputs, grid, dmax);
+    carve(s->arena, ns, nb, nc, P, host_inputs, grid, dmax, warp_teams);
     // scene cost history: kept while the batch has the same number of scenes
     if (ns > s->cost_cap) {
         if (s->d_cost) cudaFree(s->d_cost);
@@ -341,6 +353,8 @@ static int validate_config(pdc_solver* s, const pdc_config* c) {
     if (c->mu_pair_hi > c->mu_pair_lo && !(c->mu_pair_lo >= 0)) return fail(s, PDC_EINVAL, "negative mu_pair_lo");
     if (c->pcg_lanes != 0 && c->pcg_lanes != 1 && c->pcg_lanes != 2 && c->pcg_lanes != 4 && c->pcg_lanes != 8)
         return fail(s, PDC_EINVAL, "pcg_lanes not in {0, 1, 2, 4, 8}");
+    if (c->warp_max_contacts > 0 && c->warp_max_bodies > kWarpMaxBodies)
+        return fail(s, PDC_EINVAL, "warp_max_bodies above 64");
     if (c->sparse_max_bodies < 0 || c->sparse_max_bodies > pdc::kSparseMax)
         return fail(s, PDC_EINVAL, "sparse_max_bodies out of [0, 256]");
     if (c->sparse_max_bodies_large < 0 || c->sparse_max_bodies_large > pdc::kSparseMaxLarge)
@@ -380,7 +394,7 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
         cudaGetLastError();
         g_create_error = std::string("CUDA set-up failed: ") + cudaGetErrorString(e);
         pdc_destroy(s);
-        return PDC_ECUDA;
+        return e == cudaErrorMemoryAllocation ? PDC_ENOMEM : PDC_ECUDA;
     }
     if (s->blocks_per_sm < 1) s->blocks_per_sm = 1;
     {  // cooperative grid for large scenes: every block co-resident
@@ -394,7 +408,7 @@ extern "C" int pdc_create(const pdc_config* cfg, pdc_solver** out) {
             cudaGetLastError();
             g_create_error = std::string("CUDA set-up failed: ") + cudaGetErrorString(e);
             pdc_destroy(s);
-            return PDC_ECUDA;
+            return e == cudaErrorMemoryAllocation ? PDC_ENOMEM : PDC_ECUDA;
         }
         char* g = static_cast<char*>(s->d_grid);
         s->gsync.count = reinterpret_cast<unsigned int*>(g);
@@ -666,7 +680,9 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
                                      const pdc_contacts_soa* c, double* dvel, double* dang_vel,
                                      double* local_force, pdc_stats* stats, void* stream) {
     if (!s) return PDC_EINVAL;
-    if (!batch || !b || !c || !dvel || !dang_vel || !local_force) return fail(s, PDC_EINVAL, "null argument");
+    if (!batch || !b || !c) return fail(s, PDC_EINVAL, "null argument");
+    if ((b->n > 0 && (!dvel || !dang_vel)) || (c->n > 0 && !local_force))
+        return fail(s, PDC_EINVAL, "null output array");  // empty arrays may be null
     if (batch->n_scenes < 0 || b->n < 0 || c->n < 0) return fail(s, PDC_EINVAL, "negative size");
     CK(cudaSetDevice(s->device), "cudaSetDevice");
     pdc::BatchPtrs P;
@@ -693,7 +709,8 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
     P.dang = dang_vel;
     P.lforce = local_force;
     P.stats = stats;
-    if (!P.is_static || !P.depth) return fail(s, PDC_EINVAL, "device path needs is_static and depth arrays");
+    if ((b->n > 0 && !P.is_static) || (c->n > 0 && !P.depth))
+        return fail(s, PDC_EINVAL, "device path needs is_static and depth arrays");
     // NULL is the legacy default stream, as for every CUDA runtime call
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     rc = launch(s, P, st);
@@ -705,10 +722,11 @@ extern "C" int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch, cons
 extern "C" int pdc_solve_async(pdc_solver* s, double dt, const double gravity[3], const pdc_bodies_soa* bodies,
                                const pdc_contacts_soa* contacts, pdc_result* out, void* stream) {
     if (!s) return PDC_EINVAL;
-    if (!gravity || !bodies || !contacts || !out || !out->dvel || !out->dang_vel || !out->local_force)
-        return fail(s, PDC_EINVAL, "null argument");
+    if (!gravity || !bodies || !contacts || !out) return fail(s, PDC_EINVAL, "null argument");
     if (bodies->n < 0 || contacts->n < 0 || !(dt > 0)) return fail(s, PDC_EINVAL, "bad size or time step");
-    if (!bodies->is_static || !contacts->depth) return fail(s, PDC_EINVAL, "device path needs is_static and depth");
+    if ((bodies->n > 0 && (!out->dvel || !out->dang_vel || !bodies->is_static)) ||
+        (contacts->n > 0 && (!out->local_force || !contacts->depth)))
+        return fail(s, PDC_EINVAL, "null array (empty arrays may be null; is_static and depth are required)");
     CK(cudaSetDevice(s->device), "cudaSetDevice");
     pdc::BatchPtrs P;
     std::memset(&P, 0, sizeof(P));
@@ -817,7 +835,7 @@ extern "C" void pdc_host_free(void* p) {
 // solver arrays of a scene at those limits plus one full sparse-factor slot
 // (the same kSparseBlocks off-diagonal blocks a handle gives each team), so a
 // scene inside the limits takes the same branch as in pdc_solve.  Every GPU
-// that loads the library holds the 3 MiB array until the process exits.  All
+// that loads the library holds the 12 MiB array until the process exits.  All
 // calls share it and it keeps the last call's contents: the planner kernel
 // resets the work counters and each solve initialises every scratch value it
 // reads, so nothing needs clearing between calls -- but calls that overlap on
@@ -830,7 +848,7 @@ namespace {
 constexpr int kNoAllocMaxBodies = 256;
 constexpr int kNoAllocMaxContacts = 2048;
 constexpr long long kNoAllocSparseDoubles = kSparseHeaderDoubles + 36LL * kSparseBlocks;  // one team slot
-constexpr long long kNoAllocDoubles = 393216;                                              // 3 MiB
+constexpr long long kNoAllocDoubles = 1572864;                                             // 12 MiB
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
@@ -892,7 +910,7 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
     Arena A;
     A.base = base;
     A.cap = kNoAllocDoubles * sizeof(double);
-    const size_t used = carve(A, 1, std::max(bodies->n, 1), std::max(contacts->n, 1), &P, false, 1, 0);
+    const size_t used = carve(A, 1, std::max(bodies->n, 1), std::max(contacts->n, 1), &P, false, 1, 0, false);
     const size_t sparse_off = (used + 255) & ~size_t(255);
     if (sparse_off + kNoAllocSparseDoubles * sizeof(double) > A.cap)
         return fail(nullptr, PDC_EINVAL, "pdc_solve_noalloc: scene exceeds the fixed scratch");

@@ -144,8 +144,10 @@ struct BatchPtrs {
     int* didx;   // dense row-block of each active body
     int* dbody;  // body of each dense row-block (scene-relative slots)
     // per-team sparse-factorisation scratch (see SceneSolver::sparse_ws)
-    double* dense;
+    double* dense;             // one slot per thread-block team (slot = block index)
     long long dense_stride;
+    double* dense_warp;        // one slot per warp team (null: warp teams off)
+    long long dense_stride_warp;
     // one slot for the large-scene teams (nullptr: they use PCG throughout)
     double* sparse_big = nullptr;
     long long sparse_big_doubles = 0;
@@ -160,7 +162,15 @@ struct BatchPtrs {
 // sparse direct solve: nodes per scene (bitset width)
 constexpr int kSparseMax = 256;
 constexpr int kSparseWords = kSparseMax / 32;
-constexpr int kRowCap = 3072;  // off-diagonal factor blocks per scene
+// off-diagonal factor blocks per scene: every pair of the kSparseMax nodes, so
+// the direct branch never leaves the factor for lack of room (a settled heap of
+// 256 boxes fills in to several thousand blocks)
+constexpr int kRowCap = kSparseMax * (kSparseMax - 1) / 2;
+// bytes of a slot's fixed part (bitsets, index arrays, node blocks and vectors;
+// the layout of SceneSolver::sparse_ws), before its off-diagonal blocks
+constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL * kSparseMax + 3LL * (kSparseMax + 8) +
+                                                kRowCap + 8) +
+                                         8LL * (2 * 36 + 4 * 6) * kSparseMax;
 
 // The large-scene teams (whole GPU, one cluster) solve one scene per launch and
 // factor up to kSparseMaxLarge active bodies: the whole direct branch, which
@@ -462,7 +472,8 @@ class SceneSolver {
         // analogue, :385-394): compact node numbering + symbolic factorisation
         {
             const int dmax = kLargeTeam ? C.dense_max_large : C.dense_max;
-            const bool ws = kLargeTeam ? B.sparse_big != nullptr : B.dense != nullptr;
+            const bool ws = kLargeTeam ? B.sparse_big != nullptr
+                                       : (Team::kind == 1 ? B.dense_warp != nullptr : B.dense != nullptr);
             dense_mode = ws && n_local < C.direct_threshold && dmax > 0 && n_active <= dmax &&
                          n_active > 0 && dmax <= kSpMax;
         }
@@ -1122,7 +1133,13 @@ class SceneSolver {
             S.cap = left > 0 ? (int)min(left / 36, (long long)kRowCapLarge) : 0;
             return S;
         }
-        char* p = reinterpret_cast<char*>(B.dense + (long long)T.slot * B.dense_stride);
+        // thread-block teams use slot blockIdx.x of B.dense, warp teams slot
+        // (T.slot - gridDim.x) of B.dense_warp
+        const bool warp_slot = Team::kind == 1;
+        double* const base = warp_slot ? B.dense_warp + (long long)(T.slot - (int)gridDim.x) * B.dense_stride_warp
+                                       : B.dense + (long long)T.slot * B.dense_stride;
+        const long long stride = warp_slot ? B.dense_stride_warp : B.dense_stride;
+        char* p = reinterpret_cast<char*>(base);
         Sparse S;
         S.adj = reinterpret_cast<uint32_t*>(p);
         p += kSparseMax * kSparseWords * 4;
@@ -1157,8 +1174,8 @@ class SceneSolver {
         S.x = reinterpret_cast<double*>(p);
         p += kSparseMax * 6 * 8;
         S.L = reinterpret_cast<double*>(p);
-        const long long used = (p - reinterpret_cast<char*>(B.dense + (long long)T.slot * B.dense_stride)) / 8;
-        S.cap = (int)((B.dense_stride - used) / 36);
+        const long long used = (p - reinterpret_cast<char*>(base)) / 8;
+        S.cap = (int)((stride - used) / 36);
         return S;
     }
     // rank of node u among the set bits of a column pattern (= its block slot)

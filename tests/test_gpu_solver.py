@@ -229,7 +229,7 @@ def test_warp_teams_match_block_teams(gpu):
     sc = [scenes.box_columns(k + 1, 2, seed=300 + k, vel_noise=0.01, tilt=0.0) for k in range(10)]
     batch = abi.HostBatch(sc, 0.01, (0, 0, -9.81))
     blk = gpu.Solver(abi.default_config(tol=1e-8)).batch_solve(batch)
-    wrp = gpu.Solver(abi.default_config(tol=1e-8, warp_max_contacts=4096, warp_max_bodies=512)).batch_solve(batch)
+    wrp = gpu.Solver(abi.default_config(tol=1e-8, warp_max_contacts=4096, warp_max_bodies=64)).batch_solve(batch)
     assert all(s["team"] == 1 for s in wrp[3]) and all(s["team"] == 0 for s in blk[3])
     for k in range(len(sc)):
         b0, b1 = batch.body_offsets[k], batch.body_offsets[k + 1]
