@@ -211,6 +211,32 @@ def parity_vs_cpu(batch, gpu, ora, k_max):
             "newton_iter_diff_max": int(max(it)), "bar": 1e-9}
 
 
+def oracle_self_spread(batch, cfg, ora, cores, k_max):
+    """The oracle against itself on the same scenes with each scene's contacts
+    permuted: the spread that summation order alone causes in the reference
+    algorithm (the same per-scene measures as parity_vs_cpu)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib  # the reference algorithm's CPU implementation (checker only)
+
+    rng = np.random.default_rng(1)
+    perms, sc = [], []
+    for s in batch.scenes:
+        p = rng.permutation(s.n_contacts)
+        perms.append(p)
+        sc.append(abi.HostScene(s.vel, s.ang_vel, s.mass, s.inertia, s.inv_inertia, s.is_static, s.body[p],
+                                s.frame[p], s.arm[p], s.depth[p]))
+    pb = abi.HostBatch(sc, 0.0, (0.0, 0.0, 0.0))
+    pb.dt, pb.gravity = batch.dt, batch.gravity
+    o = oracle_lib.batch_solve(pb, cfg=cfg, scene_parallel=1, nthreads=cores)
+    lf = o[2].copy()
+    for k, p in enumerate(perms):
+        c0 = batch.contact_offsets[k]
+        lf[c0 + p] = o[2][c0:c0 + len(p)]
+    r = parity_vs_cpu(batch, (o[0], o[1], lf, o[3]), ora, k_max)
+    r.pop("bar", None)
+    return r
+
+
 def host_result(dev):
     """A DeviceBatch's outputs as host arrays and a stats list."""
     return (dev.out_dvel.cpu().numpy(), dev.out_dang.cpu().numpy(), dev.out_lf.cpu().numpy(), dev.stats_list())
@@ -379,15 +405,18 @@ def time_solves(lib, torch, stream, cfg, devs):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) / 1e3)
         stats.append(d.stats_list())
+    t = solver.timings()  # device time summed over scenes: set-up + build / linear solve / line search
     solver.close()
-    return times, stats
+    total = max(t["force"], 1e-30)
+    split = {k: t[k] / total for k in ("build", "solve", "line_search")}
+    return times, stats, split
 
 
 def run_world_legs(args, lib, torch, stream, local, rank, world, exported, cfg, cores, line):
     dev = f"cuda:{local}"
     devs = [lib.DeviceBatch(hb, device=dev) for hb in exported]
     # the solve kernel alone on the world's next contact sets: its roofline
-    times, stats = time_solves(lib, torch, stream, cfg, devs)
+    times, stats, split = time_solves(lib, torch, stream, cfg, devs)
     ab = [algorithmic_bytes(s) for s in stats]
     achieved = float(np.mean([a / t for a, t in zip(ab, times)])) / 1e9
     peak, peak_kind = load_peaks()
@@ -398,13 +427,14 @@ def run_world_legs(args, lib, torch, stream, local, rank, world, exported, cfg, 
                           "this workload (profiles/)" if TRAFFIC_PER_LAUNCH else "not captured for this build",
         "algorithmic_bytes_per_launch": float(np.mean(ab)), "launch_ms": float(np.mean(times)) * 1e3,
         "kernel": "solve_scenes_kernel (with its planner launch), on the world's next contact sets",
-        "solve_share_of_step": float(np.mean(times)) * 1e3 / line["ms_per_step"]}
+        "solve_share_of_step": float(np.mean(times)) * 1e3 / line["ms_per_step"],
+        "scene_time_split": split}
     ref_idx = 1
     gpu_ref = host_result(devs[ref_idx])  # FP64 outputs, kept before the mixed solves overwrite them
     # mixed precision (FP32 bulk + FP64 refinement) on the same contact sets
     mcfg = abi.default_config(**{n: getattr(cfg, n) for n, _ in abi.Config._fields_})
     mcfg.precision = abi.PDC_PRECISION_MIXED
-    mtimes, mstats = time_solves(lib, torch, stream, mcfg, devs)
+    mtimes, mstats, _ = time_solves(lib, torch, stream, mcfg, devs)
     mixed_out = host_result(devs[-1])  # the last set's mixed outputs
     line["mixed"] = {"value": args.scenes * world / max_over_ranks(float(np.mean(mtimes)), world, dev),
                      "unit": METRIC + " (solve only)", "fp64_value": args.scenes * world / max_over_ranks(
@@ -447,6 +477,9 @@ def run_world_legs(args, lib, torch, stream, local, rank, world, exported, cfg, 
                                 "sample": f"solve of the first {k_max} scenes' contact sets of one step after the "
                                           f"timed window, one scene per thread"}
         line["parity_vs_cpu"] = parity_vs_cpu(exported[ref_idx], gpu, ora, k_max)
+        # the reference algorithm's own spread on the same scenes: the oracle
+        # against itself with every scene's contacts in a permuted order
+        line["parity_vs_cpu"]["oracle_vs_permuted_oracle"] = oracle_self_spread(sub, cfg, ora, cores, k_max)
         last = len(exported) - 1
         sub_l = sub_batch(exported[last], k_max)
         ora_l = oracle_lib.batch_solve(sub_l, cfg=cfg, scene_parallel=1, nthreads=cores)
@@ -606,7 +639,7 @@ def main():
     ap.add_argument("--settle", type=int, default=245,
                     help="untimed steps before the warm-up (the timed window starts at settle + warmup)")
     ap.add_argument("--export", type=int, default=4, help="contact sets exported after the windows (>= 2)")
-    ap.add_argument("--single-sample", type=int, default=256)
+    ap.add_argument("--single-sample", type=int, default=64)
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-piles", action="store_true")

@@ -168,9 +168,14 @@ constexpr int kSparseWords = kSparseMax / 32;
 constexpr int kRowCap = kSparseMax * (kSparseMax - 1) / 2;
 // bytes of a slot's fixed part (bitsets, index arrays, node blocks and vectors;
 // the layout of SceneSolver::sparse_ws), before its off-diagonal blocks
-constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL * kSparseMax + 3LL * (kSparseMax + 8) +
+constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL * kSparseMax + 5LL * (kSparseMax + 8) +
                                                 kRowCap + 8) +
                                          8LL * (2 * 36 + 4 * 6) * kSparseMax;
+// An elimination level of the block team's factor is "fat" when one of its
+// columns takes more than kFatWork 6x6 block products (the sum of the pattern
+// sizes of the columns in its row list): such levels spread every column's
+// block rows over the team instead of one thread per column.
+constexpr int kFatWork = 24;
 
 // The large-scene teams (whole GPU, one cluster) solve one scene per launch and
 // factor up to kSparseMaxLarge active bodies: the whole direct branch, which
@@ -1081,6 +1086,8 @@ class SceneSolver {
         int* height;     // [kSparseMax] elimination-tree height of each node
         int* lvl_start;  // [levels + 1]
         int* rowptr;     // [kSparseMax + 1] row lists: columns d with L(v, d) != 0
+        int* rowbase;    // [kSparseMax + 1] block team: first block row of each lvl_nodes position
+        int* lvl_mode;   // [levels] block team: 1 = fat level
         int* rowidx;     // [kRowCap]
         int* meta;       // [0] number of levels
         double* Dg;      // [kSparseMax][36] diagonal blocks
@@ -1156,6 +1163,10 @@ class SceneSolver {
         S.lvl_start = reinterpret_cast<int*>(p);
         p += (kSparseMax + 8) * 4;
         S.rowptr = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.rowbase = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.lvl_mode = reinterpret_cast<int*>(p);
         p += (kSparseMax + 8) * 4;
         S.rowidx = reinterpret_cast<int*>(p);
         p += kRowCap * 4;
@@ -1300,6 +1311,24 @@ class SceneSolver {
                     for (int k = 0; k < n; ++k)
                         if (S.height[S.perm[k]] == l) S.lvl_nodes[pos++] = S.perm[k];
                 S.meta[0] = nlev;
+                // block rows of every column (6 per pattern block + 6 diagonal
+                // rows), in level order, and the fat levels
+                int rows = 0;
+                for (int l = 0; l < nlev; ++l) S.lvl_mode[l] = 0;
+                for (int q = 0; q < n; ++q) {
+                    const int v = S.lvl_nodes[q];
+                    int m = 0;
+                    for (int w = 0; w < kSparseWords; ++w) m += __popc(S.adj[v * kSparseWords + w]);
+                    S.rowbase[q] = rows;
+                    rows += 6 * (m + 1);
+                    int work = 0;
+                    for (int k = S.rowptr[v]; k < S.rowptr[v + 1]; ++k) {
+                        const int d = S.rowidx[k];
+                        for (int w = 0; w < kSparseWords; ++w) work += __popc(S.adj[d * kSparseWords + w]);
+                    }
+                    if (work > kFatWork) S.lvl_mode[S.height[v]] = 1;
+                }
+                S.rowbase[n] = rows;
             }
         }
         T.sync();
@@ -1637,6 +1666,143 @@ class SceneSolver {
     // of short stacks takes as many sequential steps as its tallest stack.
     // Stands in for the direct branch's SimplicialLDLT (:385-394).  Writes du;
     // false on a non-SPD pivot.
+    // Fat level of the block team's factor: the level's block rows (6 per
+    // pattern block and 6 diagonal rows per column, numbered by S.rowbase) are
+    // spread over the team.  Row r of target block L(u, v) (or of the diagonal
+    // block) takes the updates of every column d of v's row list whose pattern
+    // holds u, in row-list order -- the same sums, in the same order, as the
+    // one-thread-per-column code; then each column's diagonal block is factored,
+    // then its rows are scaled by L_vv^-T.
+    __device__ __forceinline__ int factor_level_rows(int l) {
+        const Sparse S = sparse_ws();
+        int bad = 0;
+        const int q0 = S.lvl_start[l], q1 = S.lvl_start[l + 1];
+        const int base = S.rowbase[q0], items = S.rowbase[q1] - base;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {  // diagonal blocks of the level, one thread per column
+                T.sync();
+                for (int q = q0 + tid; q < q1; q += nt) {
+                    const int v = S.lvl_nodes[q];
+                    double D[36], Lvv[36], Li[6];
+                    for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
+                    if (!chol6(D, Lvv, Li)) {
+                        bad = 1;
+                        continue;
+                    }
+                    for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
+                    for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
+                }
+                T.sync();
+            }
+            for (int t = tid; t < items; t += nt) {
+                int lo = q0, hi = q1 - 1;  // the position q with rowbase[q] <= base + t < rowbase[q + 1]
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.rowbase[mid] - base <= t) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int v = S.lvl_nodes[lo];
+                const int loc = t - (S.rowbase[lo] - base);
+                const int a = loc / 6, r = loc - 6 * a;
+                const int m = (S.rowbase[lo + 1] - S.rowbase[lo]) / 6 - 1;
+                const bool diag = a == m;
+                if (pass == 1) {
+                    if (diag) continue;
+                    double* row = S.L + 36LL * (S.cstart[v] + a) + 6 * r;
+                    double out[6];
+                    lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, row, out);
+                    for (int c = 0; c < 6; ++c) row[c] = out[c];
+                    continue;
+                }
+                const uint32_t* av = S.adj + v * kSpWords;
+                const int u = diag ? v : bit_select(av, a);
+                double* dst = diag ? S.Dg + 36 * v + 6 * r : S.L + 36LL * (S.cstart[v] + a) + 6 * r;
+                double acc[6];
+                for (int c = 0; c < 6; ++c) acc[c] = dst[c];
+                for (int k = S.rowptr[v]; k < S.rowptr[v + 1]; ++k) {
+                    const int d = S.rowidx[k];
+                    const uint32_t* ad = S.adj + d * kSpWords;
+                    if (!diag && !((ad[u >> 5] >> (u & 31)) & 1u)) continue;
+                    const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(ad, v));
+                    const double* Lud = diag ? Lvd : S.L + 36LL * (S.cstart[d] + bit_rank(ad, u));
+                    double x[6];
+#pragma unroll
+                    for (int p = 0; p < 6; ++p) x[p] = Lud[6 * r + p];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        double tt = 0.0;
+#pragma unroll
+                        for (int p = 0; p < 6; ++p) tt += x[p] * Lvd[6 * c + p];
+                        acc[c] -= tt;
+                    }
+                }
+                for (int c = 0; c < 6; ++c) dst[c] = acc[c];
+            }
+        }
+        return bad;
+    }
+
+    // Forward substitution of a fat level: a warp per column, the lanes
+    // splitting the column's row list, partials summed by a fixed shuffle tree.
+    __device__ __forceinline__ void forward_level_warp(int l) {
+        const Sparse S = sparse_ws();
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+        for (int q = S.lvl_start[l] + warp; q < S.lvl_start[l + 1]; q += nwarp) {
+            const int v = S.lvl_nodes[q];
+            double s6[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = S.rowptr[v] + lane; k < S.rowptr[v + 1]; k += 32) {
+                const int d = S.rowidx[k];
+                const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSpWords, v));
+                const double* yd = S.y + 6 * d;
+                for (int i = 0; i < 6; ++i) {
+                    double t = 0.0;
+                    for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
+                    s6[i] += t;
+                }
+            }
+            warp_sum6(s6);
+            if (lane == 0) {
+                const int gb = B.dbody[b0 + v];
+                double b6[6], yv[6];
+                for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r] - s6[r];
+                lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
+                for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
+            }
+        }
+    }
+    // Backward substitution of a fat level: a warp per column, the lanes
+    // splitting the column's pattern blocks.
+    __device__ __forceinline__ void backward_level_warp(int l) {
+        const Sparse S = sparse_ws();
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+        for (int q = S.lvl_start[l] + warp; q < S.lvl_start[l + 1]; q += nwarp) {
+            const int v = S.lvl_nodes[q];
+            const uint32_t* av = S.adj + v * kSpWords;
+            const double* colv = S.L + 36LL * S.cstart[v];
+            const int m = (S.rowbase[q + 1] - S.rowbase[q]) / 6 - 1;
+            double s6[6] = {0, 0, 0, 0, 0, 0};
+            for (int a = lane; a < m; a += 32) {
+                const int u = bit_select(av, a);
+                const double* blk = colv + 36 * a;
+                const double* xu = S.x + 6 * u;
+                for (int c = 0; c < 6; ++c) {
+                    double t = 0.0;
+                    for (int r = 0; r < 6; ++r) t += blk[6 * r + c] * xu[r];
+                    s6[c] += t;
+                }
+            }
+            warp_sum6(s6);
+            if (lane == 0) {
+                double r6[6], xv[6];
+                for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r] - s6[r];
+                ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
+                for (int r = 0; r < 6; ++r) S.x[6 * v + r] = xv[r];
+                const int gb = B.dbody[b0 + v];
+                for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = xv[r];
+            }
+        }
+    }
+
     __device__ bool dense_solve() {
         if constexpr (kLargeTeam) return dense_solve_warp();
         Sparse S = sparse_ws();
@@ -1644,6 +1810,11 @@ class SceneSolver {
         const int nlev = S.meta[0];
         int bad = 0;
         for (int l = 0; l < nlev; ++l) {
+            if (S.lvl_mode[l]) {
+                bad |= factor_level_rows(l);
+                T.sync();
+                continue;
+            }
             for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
                 const int v = S.lvl_nodes[q];
                 const uint32_t* av = S.adj + v * kSpWords;
@@ -1695,6 +1866,11 @@ class SceneSolver {
         }
         if (!bad) {
             for (int l = 0; l < nlev; ++l) {  // forward: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
+                if (S.lvl_mode[l]) {
+                    forward_level_warp(l);
+                    T.sync();
+                    continue;
+                }
                 for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
                     const int v = S.lvl_nodes[q];
                     const int gb = B.dbody[b0 + v];
@@ -1716,6 +1892,11 @@ class SceneSolver {
                 T.sync();
             }
             for (int l = nlev - 1; l >= 0; --l) {  // backward: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
+                if (S.lvl_mode[l]) {
+                    backward_level_warp(l);
+                    T.sync();
+                    continue;
+                }
                 for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
                     const int v = S.lvl_nodes[q];
                     const uint32_t* av = S.adj + v * kSpWords;
