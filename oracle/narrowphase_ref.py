@@ -95,6 +95,9 @@ def _clip(poly, u, o, lim, s):
     return out
 
 
+TIE_TOL = 1e-12  # relative tolerance under which two separating-axis candidates count as tied
+
+
 def box_box(ca, Ra, ha, cb, Rb, hb):
     dc = cb - ca
     axes, pen, valid = [], [], []
@@ -119,11 +122,15 @@ def box_box(ca, Ra, ha, cb, Rb, hb):
         pen[a] = ra + rb - abs(dc @ L)
         if pen[a] < 0:
             return []
-    bf = min(range(6), key=lambda a: (pen[a], a))
+    # ties (within TIE_TOL relative to the boxes' size) resolved by axis index
+    hmax = max(max(ha), max(hb))
+    mf = min(pen[:6])
+    bf = next(a for a in range(6) if pen[a] <= mf + TIE_TOL * (abs(mf) + hmax))
     be = -1
-    for a in range(6, 15):
-        if valid[a] and (be < 0 or pen[a] < pen[be]):
-            be = a
+    ve = [pen[a] for a in range(6, 15) if valid[a]]
+    if ve:
+        me = min(ve)
+        be = next(a for a in range(6, 15) if valid[a] and pen[a] <= me + TIE_TOL * (abs(me) + hmax))
     edge = be >= 0 and pen[be] < 0.95 * pen[bf] - 1e-9
     axis = be if edge else bf
     n = axes[axis].copy()
@@ -154,13 +161,16 @@ def box_box(ca, Ra, ha, cb, Rb, hb):
     fc = cR + hR[kf] * nref
     ku, kv = (kf + 1) % 3, (kf + 2) % 3
     u, v = RR[:, ku], RR[:, kv]
-    ki, bestd, sgn = 0, 2.0, 1.0
+    dds = [RI[:, k] @ nref for k in range(3)]
+    dmin = min(min(dd, -dd) for dd in dds)
+    ki, sgn = -1, 1.0
     for k in range(3):
-        dd = RI[:, k] @ nref
-        if dd < bestd:
-            bestd, ki, sgn = dd, k, 1.0
-        if -dd < bestd:
-            bestd, ki, sgn = -dd, k, -1.0
+        if dds[k] <= dmin + TIE_TOL:
+            ki, sgn = k, 1.0
+            break
+        if -dds[k] <= dmin + TIE_TOL:
+            ki, sgn = k, -1.0
+            break
     ic = cI + sgn * hI[ki] * RI[:, ki]
     ia, ib = (ki + 1) % 3, (ki + 2) % 3
     ea, eb = hI[ia] * RI[:, ia], hI[ib] * RI[:, ib]

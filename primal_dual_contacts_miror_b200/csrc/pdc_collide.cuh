@@ -155,6 +155,9 @@ __device__ inline int clip_side(const d3* in, int n, d3* out, d3 u, double o, do
 // Box-box: separating-axis test over 15 axes (face axes preferred unless an
 // edge axis penetrates clearly less), face clipping or edge-edge closest points.
 // Normal from A to B.  Returns the number of points (<= 4).
+// relative tolerance under which two separating-axis candidates count as tied
+constexpr double kTieTol = 1e-12;
+
 __device__ inline int box_box(const BoxG& A, const BoxG& B, CPoint* pts) {
     const d3 dc = sub3(B.c, A.c);
     d3 ax[15];
@@ -182,12 +185,23 @@ __device__ inline int box_box(const BoxG& A, const BoxG& B, CPoint* pts) {
         pen[a] = ra + rb - fabs(dot3(dc, L));
         if (pen[a] < 0) return 0;  // separating axis
     }
+    // Axis choice with ties resolved by index: among the axes whose
+    // penetration is within kTieTol (relative to the boxes' size) of the
+    // smallest, the first.  Geometric ties (equal boxes aligned face to face)
+    // otherwise fall to last-bit rounding, which differs between evaluation
+    // orders.
+    double hmax = 0;
+    for (int k = 0; k < 3; ++k) hmax = fmax(hmax, fmax(A.h[k], B.h[k]));
+    double mf = pen[0];
+    for (int a = 1; a < 6; ++a) mf = fmin(mf, pen[a]);
     int best_face = 0;
-    for (int a = 1; a < 6; ++a)
-        if (pen[a] < pen[best_face]) best_face = a;
-    int best_edge = -1;
+    while (pen[best_face] > mf + kTieTol * (fabs(mf) + hmax)) ++best_face;
+    double me = 1e300;
     for (int a = 6; a < 15; ++a)
-        if (valid[a] && (best_edge < 0 || pen[a] < pen[best_edge])) best_edge = a;
+        if (valid[a]) me = fmin(me, pen[a]);
+    int best_edge = -1;
+    for (int a = 6; a < 15 && best_edge < 0; ++a)
+        if (valid[a] && pen[a] <= me + kTieTol * (fabs(me) + hmax)) best_edge = a;
     const bool edge = best_edge >= 0 && pen[best_edge] < 0.95 * pen[best_face] - 1e-9;
     const int axis = edge ? best_edge : best_face;
     d3 n = ax[axis];
@@ -222,14 +236,18 @@ __device__ inline int box_box(const BoxG& A, const BoxG& B, CPoint* pts) {
     const d3 fc = add3(Rf.c, scl3(Rf.h[kf], nref));
     const int ku = (kf + 1) % 3, kv = (kf + 2) % 3;
     const d3 u = col(Rf.R, ku), v = col(Rf.R, kv);
-    // incident face: most anti-parallel to nref
-    int ki = 0;
-    double bestd = 2;
-    double sgn = 1;
+    // incident face: most anti-parallel to nref (first of those within kTieTol)
+    double dmin_ = 2;
     for (int k = 0; k < 3; ++k) {
         const double dd = dot3(col(In.R, k), nref);
-        if (dd < bestd) { bestd = dd; ki = k; sgn = 1; }
-        if (-dd < bestd) { bestd = -dd; ki = k; sgn = -1; }
+        dmin_ = fmin(dmin_, fmin(dd, -dd));
+    }
+    int ki = -1;
+    double sgn = 1;
+    for (int k = 0; k < 3 && ki < 0; ++k) {
+        const double dd = dot3(col(In.R, k), nref);
+        if (dd <= dmin_ + kTieTol) { ki = k; sgn = 1; }
+        else if (-dd <= dmin_ + kTieTol) { ki = k; sgn = -1; }
     }
     const d3 ic = add3(In.c, scl3(sgn * In.h[ki], col(In.R, ki)));
     const int ia = (ki + 1) % 3, ib = (ki + 2) % 3;
