@@ -168,7 +168,7 @@ constexpr int kSparseWords = kSparseMax / 32;
 constexpr int kRowCap = kSparseMax * (kSparseMax - 1) / 2;
 // bytes of a slot's fixed part (bitsets, index arrays, node blocks and vectors;
 // the layout of SceneSolver::sparse_ws), before its off-diagonal blocks
-constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL * kSparseMax + 5LL * (kSparseMax + 8) +
+constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL * kSparseMax + 10LL * (kSparseMax + 8) +
                                                 kRowCap + 8) +
                                          8LL * (2 * 36 + 4 * 6) * kSparseMax;
 // An elimination level of the block team's factor is "fat" when one of its
@@ -176,6 +176,11 @@ constexpr long long kSparseHeaderBytes = 4LL * (kSparseMax * kSparseWords + 6LL 
 // sizes of the columns in its row list): such levels spread every column's
 // block rows over the team instead of one thread per column.
 constexpr int kFatWork = 24;
+// Bottom subtrees of the block team's elimination tree whose columns take at
+// most kSubWork block products in all are factored and swept by one thread
+// each, in elimination order, with no barrier; the nodes above them are
+// scheduled level by level.
+constexpr int kSubWork = 64;
 
 // The large-scene teams (whole GPU, one cluster) solve one scene per launch and
 // factor up to kSparseMaxLarge active bodies: the whole direct branch, which
@@ -1088,6 +1093,11 @@ class SceneSolver {
         int* rowptr;     // [kSparseMax + 1] row lists: columns d with L(v, d) != 0
         int* rowbase;    // [kSparseMax + 1] block team: first block row of each lvl_nodes position
         int* lvl_mode;   // [levels] block team: 1 = fat level
+        int* sub_start;  // [team size + 1] block team: each thread's range of sub_nodes
+        int* sub_nodes;  // bottom-subtree nodes, grouped by thread, in elimination order
+        int* etp;        // elimination-tree parent (-1: root)
+        int* swork;      // subtree work (block products)
+        int* thr;        // thread of a bottom-subtree node, -1 above them
         int* rowidx;     // [kRowCap]
         int* meta;       // [0] number of levels
         double* Dg;      // [kSparseMax][36] diagonal blocks
@@ -1167,6 +1177,16 @@ class SceneSolver {
         S.rowbase = reinterpret_cast<int*>(p);
         p += (kSparseMax + 8) * 4;
         S.lvl_mode = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.sub_start = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.sub_nodes = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.etp = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.swork = reinterpret_cast<int*>(p);
+        p += (kSparseMax + 8) * 4;
+        S.thr = reinterpret_cast<int*>(p);
         p += (kSparseMax + 8) * 4;
         S.rowidx = reinterpret_cast<int*>(p);
         p += kRowCap * 4;
@@ -1293,42 +1313,91 @@ class SceneSolver {
                         }
                     }
                 }
-                // elimination-tree heights: a column can be factorised once every
-                // column that updates it is done; equal heights are independent
-                int nlev = 0;
+                // elimination tree, column work (block products, the sum of the
+                // pattern sizes over the row list) and subtree work
                 for (int k = 0; k < n; ++k) {
                     const int v = S.perm[k];
+                    int par = -1, best = n;
+                    for (int w = 0; w < kSparseWords; ++w) {
+                        uint32_t bits = S.adj[v * kSparseWords + w];
+                        while (bits) {
+                            const int u = (w << 5) + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (S.ipos[u] < best) { best = S.ipos[u]; par = u; }
+                        }
+                    }
+                    S.etp[v] = par;
+                    int work = 1;
+                    for (int q = S.rowptr[v]; q < S.rowptr[v + 1]; ++q) {
+                        const int d = S.rowidx[q];
+                        for (int w = 0; w < kSparseWords; ++w) work += __popc(S.adj[d * kSparseWords + w]);
+                    }
+                    S.height[v] = work;  // column work, for now
+                    S.swork[v] = 0;
+                }
+                for (int k = 0; k < n; ++k) {  // children before parents
+                    const int v = S.perm[k];
+                    S.swork[v] += S.height[v];
+                    if (S.etp[v] >= 0) S.swork[S.etp[v]] += S.swork[v];
+                }
+                // bottom subtrees (subtree work <= kSubWork) to threads, round
+                // robin by root in elimination order; thr = -1 above them
+                int rr = 0;
+                for (int k = n - 1; k >= 0; --k) {  // parents before children
+                    const int v = S.perm[k], par = S.etp[v];
+                    if (S.swork[v] > kSubWork) S.thr[v] = -1;
+                    else if (par < 0 || S.thr[par] < 0) S.thr[v] = (rr++) % nt;
+                    else S.thr[v] = S.thr[par];
+                }
+                for (int t = 0; t <= nt; ++t) S.sub_start[t] = 0;
+                for (int v = 0; v < n; ++v)
+                    if (S.thr[v] >= 0) S.sub_start[S.thr[v] + 1]++;
+                for (int t = 0; t < nt; ++t) S.sub_start[t + 1] += S.sub_start[t];
+                for (int t = 0; t < nt; ++t) S.lvl_start[t] = S.sub_start[t];  // fill cursors
+                for (int k = 0; k < n; ++k) {
+                    const int v = S.perm[k];
+                    if (S.thr[v] >= 0) S.sub_nodes[S.lvl_start[S.thr[v]]++] = v;
+                }
+                // levels of the nodes above the bottom subtrees: a column can be
+                // factorised once every column that updates it is done; equal
+                // heights are independent
+                int nlev = 0, ntop = 0;
+                for (int k = 0; k < n; ++k) {
+                    const int v = S.perm[k];
+                    if (S.thr[v] >= 0) continue;
+                    const int work = S.height[v];
                     int h = 0;
-                    for (int q = S.rowptr[v]; q < S.rowptr[v + 1]; ++q) h = max(h, S.height[S.rowidx[q]] + 1);
-                    S.height[v] = h;
+                    for (int q = S.rowptr[v]; q < S.rowptr[v + 1]; ++q) {
+                        const int d = S.rowidx[q];
+                        if (S.thr[d] < 0) h = max(h, S.swork[d] + 1);  // swork of a top node: its height
+                    }
+                    S.swork[v] = h;
+                    S.height[v] = work;
                     nlev = max(nlev, h + 1);
+                    ++ntop;
                 }
                 for (int l = 0; l <= nlev; ++l) S.lvl_start[l] = 0;
-                for (int v = 0; v < n; ++v) S.lvl_start[S.height[v] + 1]++;
+                for (int v = 0; v < n; ++v)
+                    if (S.thr[v] < 0) S.lvl_start[S.swork[v] + 1]++;
                 for (int l = 0; l < nlev; ++l) S.lvl_start[l + 1] += S.lvl_start[l];
                 int pos = 0;  // stable in elimination order
                 for (int l = 0; l < nlev; ++l)
                     for (int k = 0; k < n; ++k)
-                        if (S.height[S.perm[k]] == l) S.lvl_nodes[pos++] = S.perm[k];
+                        if (S.thr[S.perm[k]] < 0 && S.swork[S.perm[k]] == l) S.lvl_nodes[pos++] = S.perm[k];
                 S.meta[0] = nlev;
-                // block rows of every column (6 per pattern block + 6 diagonal
-                // rows), in level order, and the fat levels
+                // block rows of every top column (6 per pattern block + 6
+                // diagonal rows), in level order, and the fat levels
                 int rows = 0;
                 for (int l = 0; l < nlev; ++l) S.lvl_mode[l] = 0;
-                for (int q = 0; q < n; ++q) {
+                for (int q = 0; q < ntop; ++q) {
                     const int v = S.lvl_nodes[q];
                     int m = 0;
                     for (int w = 0; w < kSparseWords; ++w) m += __popc(S.adj[v * kSparseWords + w]);
                     S.rowbase[q] = rows;
                     rows += 6 * (m + 1);
-                    int work = 0;
-                    for (int k = S.rowptr[v]; k < S.rowptr[v + 1]; ++k) {
-                        const int d = S.rowidx[k];
-                        for (int w = 0; w < kSparseWords; ++w) work += __popc(S.adj[d * kSparseWords + w]);
-                    }
-                    if (work > kFatWork) S.lvl_mode[S.height[v]] = 1;
+                    if (S.height[v] - 1 > kFatWork) S.lvl_mode[S.swork[v]] = 1;
                 }
-                S.rowbase[n] = rows;
+                S.rowbase[ntop] = rows;
             }
         }
         T.sync();
@@ -1658,14 +1727,6 @@ class SceneSolver {
         }
     }
 
-    // Block Cholesky factorisation + solve of the Newton system: left-looking,
-    // one elimination-tree level at a time (columns of a level are independent;
-    // one team sync per level in each of factor / forward / backward; a
-    // non-SPD pivot only marks the scene, read once after the factorisation --
-    // later columns then compute garbage in bounded loops), so a pile
-    // of short stacks takes as many sequential steps as its tallest stack.
-    // Stands in for the direct branch's SimplicialLDLT (:385-394).  Writes du;
-    // false on a non-SPD pivot.
     // Fat level of the block team's factor: the level's block rows (6 per
     // pattern block and 6 diagonal rows per column, numbered by S.rowbase) are
     // spread over the team.  Row r of target block L(u, v) (or of the diagonal
@@ -1803,60 +1864,116 @@ class SceneSolver {
         }
     }
 
+    // One column of the factor by one thread (left-looking): D = A_vv - sum
+    // L(v,d) L(v,d)^T and L(u,v) -= L(u,d) L(v,d)^T over the columns d of v's
+    // row list, then L_vv = chol(D) and L(u,v) = A(u,v) L_vv^-T.  Returns 1 on a
+    // non-SPD pivot (the column is left unscaled).
+    __device__ __forceinline__ int factor_column(const Sparse& S, int v) const {
+        const uint32_t* av = S.adj + v * kSpWords;
+        double* colv = S.L + 36LL * S.cstart[v];
+        double D[36];
+        for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
+        for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
+            const int d = S.rowidx[r];
+            const uint32_t* ad = S.adj + d * kSpWords;
+            const double* cold = S.L + 36LL * S.cstart[d];
+            const double* Lvd = cold + 36 * bit_rank(ad, v);
+            sub_abt6(D, Lvd, Lvd);
+            int a = 0;  // walk pattern(d): u after v -> L(u,v) -= L(u,d) L(v,d)^T
+            for (int w = 0; w < spw(); ++w) {
+                uint32_t bits = ad[w];
+                while (bits) {
+                    const int u = (w << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (u != v && S.ipos[u] > S.ipos[v]) sub_abt6(colv + 36 * bit_rank(av, u), cold + 36 * a, Lvd);
+                    ++a;
+                }
+            }
+        }
+        double Lvv[36], Li[6];
+        if (!chol6(D, Lvv, Li)) return 1;
+        for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
+        for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
+        int m = 0;
+        for (int w = 0; w < spw(); ++w) m += __popc(av[w]);
+        for (int a = 0; a < m; ++a) {  // L(u,v) = A(u,v) L_vv^-T, row by row
+            double* blk = colv + 36 * a;
+            for (int r = 0; r < 6; ++r) {
+                double row[6];
+                lsolve6(Lvv, Li, blk + 6 * r, row);
+                for (int c = 0; c < 6; ++c) blk[6 * r + c] = row[c];
+            }
+        }
+        return 0;
+    }
+    // forward substitution of one column: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
+    __device__ __forceinline__ void forward_column(const Sparse& S, int v) const {
+        const int gb = B.dbody[b0 + v];
+        double b6[6], yv[6];
+        for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r];
+        for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
+            const int d = S.rowidx[r];
+            const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSpWords, v));
+            const double* yd = S.y + 6 * d;
+            for (int i = 0; i < 6; ++i) {
+                double t = 0.0;
+                for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
+                b6[i] -= t;
+            }
+        }
+        lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
+        for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
+    }
+    // backward substitution of one column: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
+    __device__ __forceinline__ void backward_column(const Sparse& S, int v) const {
+        const uint32_t* av = S.adj + v * kSpWords;
+        const double* colv = S.L + 36LL * S.cstart[v];
+        double r6[6], xv[6];
+        for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r];
+        int a = 0;
+        for (int w = 0; w < spw(); ++w) {
+            uint32_t bits = av[w];
+            while (bits) {
+                const int u = (w << 5) + __ffs(bits) - 1;
+                bits &= bits - 1;
+                const double* blk = colv + 36 * a;
+                const double* xu = S.x + 6 * u;
+                for (int c = 0; c < 6; ++c) {
+                    double t = 0.0;
+                    for (int r = 0; r < 6; ++r) t += blk[6 * r + c] * xu[r];
+                    r6[c] -= t;
+                }
+                ++a;
+            }
+        }
+        ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
+        for (int r = 0; r < 6; ++r) S.x[6 * v + r] = xv[r];
+        const int gb = B.dbody[b0 + v];
+        for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = xv[r];
+    }
+
+    // Block Cholesky factorisation + solve of the Newton system (left-looking).
+    // The bottom subtrees of the elimination tree are each factored and swept
+    // by one thread, in elimination order, with no barrier (a stack of boxes is
+    // one such chain); the columns above them go one elimination-tree level at
+    // a time (columns of a level are independent): a thin level a thread per
+    // column, a fat one its block rows over the team (factor_level_rows).  A
+    // non-SPD pivot only marks the scene, read once after the factorisation;
+    // later columns then compute garbage in bounded loops.  Stands in for the
+    // direct branch's SimplicialLDLT (:385-394).  Writes du; false on a non-SPD
+    // pivot.
     __device__ bool dense_solve() {
         if constexpr (kLargeTeam) return dense_solve_warp();
         Sparse S = sparse_ws();
-        const int n = n_active;
         const int nlev = S.meta[0];
+        const int sub0 = S.sub_start[tid], sub1 = S.sub_start[tid + 1];
         int bad = 0;
+        for (int q = sub0; q < sub1; ++q) bad |= factor_column(S, S.sub_nodes[q]);
+        T.sync();
         for (int l = 0; l < nlev; ++l) {
-            if (S.lvl_mode[l]) {
-                bad |= factor_level_rows(l);
-                T.sync();
-                continue;
-            }
-            for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
-                const int v = S.lvl_nodes[q];
-                const uint32_t* av = S.adj + v * kSpWords;
-                double* colv = S.L + 36LL * S.cstart[v];
-                double D[36];
-                for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
-                for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
-                    const int d = S.rowidx[r];
-                    const uint32_t* ad = S.adj + d * kSpWords;
-                    const double* cold = S.L + 36LL * S.cstart[d];
-                    const double* Lvd = cold + 36 * bit_rank(ad, v);
-                    sub_abt6(D, Lvd, Lvd);
-                    int a = 0;  // walk pattern(d): u after v -> L(u,v) -= L(u,d) L(v,d)^T
-                    for (int w = 0; w < spw(); ++w) {
-                        uint32_t bits = ad[w];
-                        while (bits) {
-                            const int u = (w << 5) + __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            if (u != v && S.ipos[u] > S.ipos[v])
-                                sub_abt6(colv + 36 * bit_rank(av, u), cold + 36 * a, Lvd);
-                            ++a;
-                        }
-                    }
-                }
-                double Lvv[36], Li[6];
-                if (!chol6(D, Lvv, Li)) {
-                    bad = 1;
-                    continue;
-                }
-                for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
-                for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
-                int m = 0;
-                for (int w = 0; w < spw(); ++w) m += __popc(av[w]);
-                for (int a = 0; a < m; ++a) {  // L(u,v) = A(u,v) L_vv^-T, row by row
-                    double* blk = colv + 36 * a;
-                    for (int r = 0; r < 6; ++r) {
-                        double row[6];
-                        lsolve6(Lvv, Li, blk + 6 * r, row);
-                        for (int c = 0; c < 6; ++c) blk[6 * r + c] = row[c];
-                    }
-                }
-            }
+            if (S.lvl_mode[l]) bad |= factor_level_rows(l);
+            else
+                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) bad |= factor_column(S, S.lvl_nodes[q]);
             T.sync();  // level barrier; a failed pivot is checked once after the factorisation
         }
         {
@@ -1865,69 +1982,22 @@ class SceneSolver {
             bad = fl[0] > 0;
         }
         if (!bad) {
-            for (int l = 0; l < nlev; ++l) {  // forward: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
-                if (S.lvl_mode[l]) {
-                    forward_level_warp(l);
-                    T.sync();
-                    continue;
-                }
-                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
-                    const int v = S.lvl_nodes[q];
-                    const int gb = B.dbody[b0 + v];
-                    double b6[6], yv[6];
-                    for (int r = 0; r < 6; ++r) b6[r] = B.rhs[6 * gb + r];
-                    for (int r = S.rowptr[v]; r < S.rowptr[v + 1]; ++r) {
-                        const int d = S.rowidx[r];
-                        const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSpWords, v));
-                        const double* yd = S.y + 6 * d;
-                        for (int i = 0; i < 6; ++i) {
-                            double t = 0.0;
-                            for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
-                            b6[i] -= t;
-                        }
-                    }
-                    lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
-                    for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
-                }
+            for (int q = sub0; q < sub1; ++q) forward_column(S, S.sub_nodes[q]);
+            T.sync();
+            for (int l = 0; l < nlev; ++l) {
+                if (S.lvl_mode[l]) forward_level_warp(l);
+                else
+                    for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) forward_column(S, S.lvl_nodes[q]);
                 T.sync();
             }
-            for (int l = nlev - 1; l >= 0; --l) {  // backward: x_v = L_vv^-T (y_v - sum L(u,v)^T x_u)
-                if (S.lvl_mode[l]) {
-                    backward_level_warp(l);
-                    T.sync();
-                    continue;
-                }
-                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) {
-                    const int v = S.lvl_nodes[q];
-                    const uint32_t* av = S.adj + v * kSpWords;
-                    const double* colv = S.L + 36LL * S.cstart[v];
-                    double r6[6], xv[6];
-                    for (int r = 0; r < 6; ++r) r6[r] = S.y[6 * v + r];
-                    int a = 0;
-                    for (int w = 0; w < spw(); ++w) {
-                        uint32_t bits = av[w];
-                        while (bits) {
-                            const int u = (w << 5) + __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            const double* blk = colv + 36 * a;
-                            const double* xu = S.x + 6 * u;
-                            for (int c = 0; c < 6; ++c) {
-                                double t = 0.0;
-                                for (int r = 0; r < 6; ++r) t += blk[6 * r + c] * xu[r];
-                                r6[c] -= t;
-                            }
-                            ++a;
-                        }
-                    }
-                    ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
-                    for (int r = 0; r < 6; ++r) S.x[6 * v + r] = xv[r];
-                    const int gb = B.dbody[b0 + v];
-                    for (int r = 0; r < 6; ++r) B.du[6 * gb + r] = xv[r];
-                }
+            for (int l = nlev - 1; l >= 0; --l) {
+                if (S.lvl_mode[l]) backward_level_warp(l);
+                else
+                    for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) backward_column(S, S.lvl_nodes[q]);
                 T.sync();
             }
+            for (int q = sub1 - 1; q >= sub0; --q) backward_column(S, S.sub_nodes[q]);
         }
-        (void)n;
         T.sync();
         return !bad;
     }
@@ -2728,7 +2798,7 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
 // Persistent solve: every CTA first drains the CTA queue (one scene per CTA),
 // then each of its warps drains the warp queue (one scene per warp).
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
                                                            const __grid_constant__ EngineCfg C) {
     __shared__ double s_red[2 * 8 * 32];
     __shared__ int s_int[33];
