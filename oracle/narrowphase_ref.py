@@ -10,7 +10,9 @@ sphere/box/plane tests -- and the reference's own post-processing, which it
 follows line by line:
   * pairs in (id0, id1) order, normal from the lower id to the higher
     (DynamicSystem.cpp:251-276);
-  * per pair: points sorted lexicographically by position, consecutive points
+  * per pair: points sorted lexicographically by position (each coordinate
+    on a 1e-9 m grid, ties in generation order: exact ties of axis-aligned
+    geometry must not fall to last-bit rounding), consecutive points
     closer than 1e-4 merged (summed normal renormalised, minimum depth, first
     point's position, frame rebuilt) (DynamicSystem.cpp:343-381);
   * contact frame from the normal by normalToTransform, depth = |penetration|
@@ -271,8 +273,13 @@ def pair_points(ta, ca, Ra, ha, tb, cb, Rb, hb):
     return []
 
 
+def grid_key(x):
+    """A coordinate on the 1e-9 m grid (round half to even), the sort key."""
+    return float(np.rint(float(x) * 1e9))
+
+
 def merge_points(pts):
-    pts = sorted(pts, key=lambda t: (t[0][0], t[0][1], t[0][2]))
+    pts = sorted(pts, key=lambda t: (grid_key(t[0][0]), grid_key(t[0][1]), grid_key(t[0][2])))
     out = []
     i = 0
     while i < len(pts):

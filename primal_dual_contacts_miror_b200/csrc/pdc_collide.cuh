@@ -413,15 +413,25 @@ __device__ inline int pair_points(const BodyG& a, const BodyG& b, CPoint* pts) {
     return m;
 }
 
+// Sort key of one coordinate: the coordinate on a 1e-9 m grid (round half to
+// even).  Axis-aligned geometry puts many points at mathematically equal
+// coordinates that rounding separates by a few ulps, differently in every
+// evaluation order; on the grid they tie and keep their generation order.
+__device__ __forceinline__ double grid_key(double x) { return rint(__dmul_rn(x, 1e9)); }
+
 // Lexicographic sort by position and merge of near points (DynamicSystem.cpp:343-381).
+// Positions are compared on the 1e-9 m grid (grid_key), ties in generation
+// order (a stable sort).
 __device__ inline int merge_points(CPoint* pts, int m) {
     for (int i = 1; i < m; ++i) {  // insertion sort, x then y then z
         const CPoint key = pts[i];
         int j = i - 1;
         auto less = [](const CPoint& a, const CPoint& b) {
-            if (a.p.x != b.p.x) return a.p.x < b.p.x;
-            if (a.p.y != b.p.y) return a.p.y < b.p.y;
-            return a.p.z < b.p.z;
+            const double ax = grid_key(a.p.x), bx = grid_key(b.p.x);
+            if (ax != bx) return ax < bx;
+            const double ay = grid_key(a.p.y), by = grid_key(b.p.y);
+            if (ay != by) return ay < by;
+            return grid_key(a.p.z) < grid_key(b.p.z);
         };
         while (j >= 0 && less(key, pts[j])) {
             pts[j + 1] = pts[j];

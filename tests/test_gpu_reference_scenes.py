@@ -6,10 +6,10 @@ checkout), stepped by the device world with each file's own solver settings,
 time step, gravity and adaptive stepping:
   * the four small scenes step by step against the host pipeline (numpy
     contact generation -> oracle solve -> numpy integration), every step
-    started from the same state in both (the host's, copied into the device
-    world), so that each step's contact generation, solve and integration are
-    compared and not the divergence of two chaotic trajectories (a house of
-    cards is one);
+    (every substep, with adaptive stepping) started from the same state in
+    both (the host's, copied into the device world), so that each step's
+    contact generation, solve and integration are compared and not the
+    divergence of two chaotic trajectories (a house of cards is one);
   * bricks (564 bodies) and funnel (1,607): at points along the trajectory,
     device contact generation against the numpy restatement on the same poses
     and the GPU solve of the contact set against the oracle; no non-finite
@@ -49,22 +49,42 @@ def test_small_scene_steps_match_host_pipeline(name, steps):
     w = lib.World(abi.ShapeBatch([sc], dt, g), cfg=cfg, contacts_per_body=24)
     state = world_ref.initial_state(sc)
     worst = [0.0, 0.0]
+
+    def compare(dev_world):
+        dev_world.sync()
+        pos, quat, vel, ang = dev_world.state()
+        st, ov = dev_world.stats()
+        assert ov.sum() == 0 and not st[0]["status"] & abi.PDC_SCENE_NONFINITE
+        worst[0] = max(worst[0], float(np.abs(pos - state[0]).max()))
+        worst[1] = max(worst[1], float(np.abs(np.concatenate([vel - state[2], ang - state[3]])).max()))
+
     for k in range(steps):
         w.set_state(*[np.ascontiguousarray(a) for a in state])
         w.sync()
         if sim["adaptive_timestep"]:
-            n_host = world_ref.step_adaptive(sc, state, dt, g, cfg, sim["substep_factor"])
+            # the device's substep count for this step from the host's state ...
             n_dev = w.step_adaptive(1, sim["substep_factor"])
+            # ... and every substep (contacts, solve, integration) from the same
+            # state on both sides: the substeps of one step run on without a
+            # reset, so comparing only whole steps would compare two chaotic
+            # runs of several substeps each
+            done, n_host = 0.0, 0
+            while done < 1.0:
+                h = world_ref.substep(sc, state, dt, done, sim["substep_factor"])
+                ws = lib.World(abi.ShapeBatch([sc], h * dt, g), cfg=cfg, contacts_per_body=24)
+                ws.set_state(*[np.ascontiguousarray(a) for a in state])
+                ws.sync()
+                world_ref.step(sc, state, h * dt, g, cfg)
+                ws.step(1)
+                compare(ws)
+                ws.close()
+                done += h
+                n_host += 1
             assert n_host == n_dev, (k, n_host, n_dev)
         else:
             world_ref.step(sc, state, dt, g, cfg)
             w.step(1)
-        w.sync()
-        pos, quat, vel, ang = w.state()
-        st, ov = w.stats()
-        assert ov.sum() == 0 and not st[0]["status"] & abi.PDC_SCENE_NONFINITE
-        worst[0] = max(worst[0], float(np.abs(pos - state[0]).max()))
-        worst[1] = max(worst[1], float(np.abs(np.concatenate([vel - state[2], ang - state[3]])).max()))
+            compare(w)
     vscale = max(float(np.abs(state[2]).max()), 9.81 * dt)
     assert worst[0] < 1e-9 and worst[1] < 1e-6 * vscale, (worst, vscale)
     moving = ~sc["is_static"].astype(bool)
