@@ -1340,14 +1340,29 @@ class SceneSolver {
                     S.swork[v] += S.height[v];
                     if (S.etp[v] >= 0) S.swork[S.etp[v]] += S.swork[v];
                 }
-                // bottom subtrees (subtree work <= kSubWork) to threads, round
-                // robin by root in elimination order; thr = -1 above them
-                int rr = 0;
+                // bottom subtrees (subtree work <= kSubWork) to threads; thr = -1
+                // above them.  The lanes of a warp whose subtrees take different
+                // paths run one after another, so each root goes to the warp with
+                // the least subtree work so far, on that warp's next lane
+                // (lvl_start holds the warps' work and root counts until the
+                // level pass below)
+                const int nwarp = nt >> 5;
+                int* wload = S.lvl_start;
+                int* wroots = S.lvl_start + 32;
+                for (int w = 0; w < nwarp; ++w) wload[w] = wroots[w] = 0;
                 for (int k = n - 1; k >= 0; --k) {  // parents before children
                     const int v = S.perm[k], par = S.etp[v];
-                    if (S.swork[v] > kSubWork) S.thr[v] = -1;
-                    else if (par < 0 || S.thr[par] < 0) S.thr[v] = (rr++) % nt;
-                    else S.thr[v] = S.thr[par];
+                    if (S.swork[v] > kSubWork) {
+                        S.thr[v] = -1;
+                    } else if (par < 0 || S.thr[par] < 0) {
+                        int best = 0;
+                        for (int w = 1; w < nwarp; ++w)
+                            if (wload[w] < wload[best]) best = w;
+                        wload[best] += S.swork[v];
+                        S.thr[v] = 32 * best + (wroots[best]++ & 31);
+                    } else {
+                        S.thr[v] = S.thr[par];
+                    }
                 }
                 for (int t = 0; t <= nt; ++t) S.sub_start[t] = 0;
                 for (int v = 0; v < n; ++v)
