@@ -1748,13 +1748,61 @@ class SceneSolver {
     // block) takes the updates of every column d of v's row list whose pattern
     // holds u, in row-list order -- the same sums, in the same order, as the
     // one-thread-per-column code; then each column's diagonal block is factored,
-    // then its rows are scaled by L_vv^-T.
+    // then its rows are scaled by L_vv^-T.  A level with few rows (the top of
+    // the elimination tree: one column, a long row list) gives each row
+    // `split` (2, 4 or 8) adjacent lanes that take every split-th entry of the
+    // row list and combine their partial sums by an xor butterfly (every lane
+    // gets the same bits).
     __device__ __forceinline__ int factor_level_rows(int l) {
         const Sparse S = sparse_ws();
         int bad = 0;
         const int q0 = S.lvl_start[l], q1 = S.lvl_start[l + 1];
         const int base = S.rowbase[q0], items = S.rowbase[q1] - base;
-        for (int pass = 0; pass < 2; ++pass) {
+        int split = 1;
+        while (split < 8 && items * split * 2 <= nt) split *= 2;
+        if (split > 1) {  // one round: items * split <= nt
+            const int it = tid / split, j = tid - it * split;
+            double part[6] = {0, 0, 0, 0, 0, 0};
+            double* dst = nullptr;
+            if (it < items) {
+                int lo = q0, hi = q1 - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.rowbase[mid] - base <= it) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int v = S.lvl_nodes[lo];
+                const int loc = it - (S.rowbase[lo] - base);
+                const int a = loc / 6, r = loc - 6 * a;
+                const int m = (S.rowbase[lo + 1] - S.rowbase[lo]) / 6 - 1;
+                const bool diag = a == m;
+                const int u = diag ? v : bit_select(S.adj + v * kSpWords, a);
+                dst = diag ? S.Dg + 36 * v + 6 * r : S.L + 36LL * (S.cstart[v] + a) + 6 * r;
+                for (int k = S.rowptr[v] + j; k < S.rowptr[v + 1]; k += split) {
+                    const int d = S.rowidx[k];
+                    const uint32_t* ad = S.adj + d * kSpWords;
+                    if (!diag && !((ad[u >> 5] >> (u & 31)) & 1u)) continue;
+                    const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(ad, v));
+                    const double* Lud = diag ? Lvd : S.L + 36LL * (S.cstart[d] + bit_rank(ad, u));
+                    double x[6];
+#pragma unroll
+                    for (int p = 0; p < 6; ++p) x[p] = Lud[6 * r + p];
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) {
+                        double tt = 0.0;
+#pragma unroll
+                        for (int p = 0; p < 6; ++p) tt += x[p] * Lvd[6 * c + p];
+                        part[c] += tt;
+                    }
+                }
+            }
+            for (int o = 1; o < split; o <<= 1)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) part[c] += __shfl_xor_sync(0xffffffffu, part[c], o);
+            if (dst && j == 0)
+                for (int c = 0; c < 6; ++c) dst[c] -= part[c];
+        }
+        for (int pass = split > 1 ? 1 : 0; pass < 2; ++pass) {
             if (pass == 1) {  // diagonal blocks of the level, one thread per column
                 T.sync();
                 for (int q = q0 + tid; q < q1; q += nt) {
