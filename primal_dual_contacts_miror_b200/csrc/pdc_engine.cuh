@@ -1969,6 +1969,65 @@ class SceneSolver {
         }
         return 0;
     }
+    // One column of the factor by one warp: the column's block rows (6 per
+    // pattern block, 6 for the diagonal block) over the lanes, each summing the
+    // updates of v's row list in row-list order (the sums of factor_column);
+    // lane 0 factors the diagonal block, the lanes scale the rows by L_vv^-T.
+    // Every lane returns 1 on a non-SPD pivot.
+    __device__ __forceinline__ int factor_column_warp(const Sparse& S, int v, int lane) const {
+        const uint32_t* av = S.adj + v * kSpWords;
+        int m = 0;
+        for (int w = 0; w < spw(); ++w) m += __popc(av[w]);
+        for (int t = lane; t < 6 * (m + 1); t += 32) {
+            const int a = t / 6, r = t - 6 * a;
+            const bool diag = a == m;
+            const int u = diag ? v : bit_select(av, a);
+            double* dst = diag ? S.Dg + 36 * v + 6 * r : S.L + 36LL * (S.cstart[v] + a) + 6 * r;
+            double acc[6];
+            for (int c = 0; c < 6; ++c) acc[c] = dst[c];
+            for (int k = S.rowptr[v]; k < S.rowptr[v + 1]; ++k) {
+                const int d = S.rowidx[k];
+                const uint32_t* ad = S.adj + d * kSpWords;
+                if (!diag && !((ad[u >> 5] >> (u & 31)) & 1u)) continue;
+                const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(ad, v));
+                const double* Lud = diag ? Lvd : S.L + 36LL * (S.cstart[d] + bit_rank(ad, u));
+                double x[6];
+#pragma unroll
+                for (int p = 0; p < 6; ++p) x[p] = Lud[6 * r + p];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    double tt = 0.0;
+#pragma unroll
+                    for (int p = 0; p < 6; ++p) tt += x[p] * Lvd[6 * c + p];
+                    acc[c] -= tt;
+                }
+            }
+            for (int c = 0; c < 6; ++c) dst[c] = acc[c];
+        }
+        __syncwarp();
+        int bad = 0;
+        if (lane == 0) {
+            double D[36], Lvv[36], Li[6];
+            for (int e = 0; e < 36; ++e) D[e] = S.Dg[36 * v + e];
+            if (chol6(D, Lvv, Li)) {
+                for (int e = 0; e < 36; ++e) S.Ld[36 * v + e] = Lvv[e];
+                for (int e = 0; e < 6; ++e) S.Ldi[6 * v + e] = Li[e];
+            } else {
+                bad = 1;
+            }
+        }
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        __syncwarp();
+        if (!bad)
+            for (int t = lane; t < 6 * m; t += 32) {
+                double* row = S.L + 36LL * S.cstart[v] + 6 * t;  // block t / 6, row t % 6
+                double out[6];
+                lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, row, out);
+                for (int c = 0; c < 6; ++c) row[c] = out[c];
+            }
+        __syncwarp();
+        return bad;
+    }
     // forward substitution of one column: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
     __device__ __forceinline__ void forward_column(const Sparse& S, int v) const {
         const int gb = B.dbody[b0 + v];
@@ -2016,9 +2075,11 @@ class SceneSolver {
     }
 
     // Block Cholesky factorisation + solve of the Newton system (left-looking).
-    // The bottom subtrees of the elimination tree are each factored and swept
-    // by one thread, in elimination order, with no barrier (a stack of boxes is
-    // one such chain); the columns above them go one elimination-tree level at
+    // The bottom subtrees of the elimination tree (a stack of boxes is one such
+    // chain) belong to threads, balanced over the warps; a warp factors its
+    // lanes' subtrees column by column (factor_column_warp) and each thread
+    // sweeps its own, in elimination order, with no team barrier; the columns
+    // above them go one elimination-tree level at
     // a time (columns of a level are independent): a thin level a thread per
     // column, a fat one its block rows over the team (factor_level_rows).  A
     // non-SPD pivot only marks the scene, read once after the factorisation;
@@ -2031,7 +2092,12 @@ class SceneSolver {
         const int nlev = S.meta[0];
         const int sub0 = S.sub_start[tid], sub1 = S.sub_start[tid + 1];
         int bad = 0;
-        for (int q = sub0; q < sub1; ++q) bad |= factor_column(S, S.sub_nodes[q]);
+        {  // each warp factors its lanes' subtrees, lane by lane, a warp per column
+            const int lane = tid & 31, w0 = tid - lane;
+            for (int ln = 0; ln < 32; ++ln)
+                for (int q = S.sub_start[w0 + ln]; q < S.sub_start[w0 + ln + 1]; ++q)
+                    bad |= factor_column_warp(S, S.sub_nodes[q], lane);
+        }
         T.sync();
         for (int l = 0; l < nlev; ++l) {
             if (S.lvl_mode[l]) bad |= factor_level_rows(l);
