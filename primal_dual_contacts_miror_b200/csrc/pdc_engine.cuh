@@ -2028,6 +2028,68 @@ class SceneSolver {
         __syncwarp();
         return bad;
     }
+    // Forward and backward substitution of one column by one warp: lanes 6e + i
+    // (e < 5) take the row-list entry (pattern block) e of a round of five and
+    // row i; lane i then subtracts the round's products in entry order, so each
+    // component sees the same operations in the same order as forward_column /
+    // backward_column; lane 0 applies the diagonal block.
+    __device__ __forceinline__ void forward_column_warp(const Sparse& S, int v, int lane) const {
+        const int gb = B.dbody[b0 + v];
+        const int k0 = S.rowptr[v], k1 = S.rowptr[v + 1];
+        const int e = lane / 6, i = lane - 6 * e;
+        double b = lane < 6 ? B.rhs[6 * gb + lane] : 0.0;
+        for (int kb = k0; kb < k1; kb += 5) {
+            double t = 0.0;
+            if (e < 5 && kb + e < k1) {
+                const int d = S.rowidx[kb + e];
+                const double* Lvd = S.L + 36LL * (S.cstart[d] + bit_rank(S.adj + d * kSpWords, v));
+                const double* yd = S.y + 6 * d;
+                for (int c = 0; c < 6; ++c) t += Lvd[6 * i + c] * yd[c];
+            }
+            for (int q = 0; q < 5; ++q) {
+                const double tq = __shfl_sync(0xffffffffu, t, 6 * q + i);
+                if (lane < 6 && kb + q < k1) b -= tq;
+            }
+        }
+        double b6[6];
+        for (int r = 0; r < 6; ++r) b6[r] = __shfl_sync(0xffffffffu, b, r);
+        if (lane == 0) {
+            double yv[6];
+            lsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, b6, yv);
+            for (int r = 0; r < 6; ++r) S.y[6 * v + r] = yv[r];
+        }
+        __syncwarp();
+    }
+    __device__ __forceinline__ void backward_column_warp(const Sparse& S, int v, int lane) const {
+        const uint32_t* av = S.adj + v * kSpWords;
+        const double* colv = S.L + 36LL * S.cstart[v];
+        int m = 0;
+        for (int w = 0; w < spw(); ++w) m += __popc(av[w]);
+        const int e = lane / 6, c = lane - 6 * e;
+        double r = lane < 6 ? S.y[6 * v + lane] : 0.0;
+        for (int ab = 0; ab < m; ab += 5) {
+            double t = 0.0;
+            if (e < 5 && ab + e < m) {
+                const double* blk = colv + 36 * (ab + e);
+                const double* xu = S.x + 6 * bit_select(av, ab + e);
+                for (int rr = 0; rr < 6; ++rr) t += blk[6 * rr + c] * xu[rr];
+            }
+            for (int q = 0; q < 5; ++q) {
+                const double tq = __shfl_sync(0xffffffffu, t, 6 * q + c);
+                if (lane < 6 && ab + q < m) r -= tq;
+            }
+        }
+        double r6[6];
+        for (int k = 0; k < 6; ++k) r6[k] = __shfl_sync(0xffffffffu, r, k);
+        if (lane == 0) {
+            double xv[6];
+            ltsolve6(S.Ld + 36 * v, S.Ldi + 6 * v, r6, xv);
+            for (int k = 0; k < 6; ++k) S.x[6 * v + k] = xv[k];
+            const int gb = B.dbody[b0 + v];
+            for (int k = 0; k < 6; ++k) B.du[6 * gb + k] = xv[k];
+        }
+        __syncwarp();
+    }
     // forward substitution of one column: y_v = L_vv^-1 (b_v - sum L(v,d) y_d)
     __device__ __forceinline__ void forward_column(const Sparse& S, int v) const {
         const int gb = B.dbody[b0 + v];
@@ -2080,8 +2142,9 @@ class SceneSolver {
     // lanes' subtrees column by column (factor_column_warp) and each thread
     // sweeps its own, in elimination order, with no team barrier; the columns
     // above them go one elimination-tree level at
-    // a time (columns of a level are independent): a thin level a thread per
-    // column, a fat one its block rows over the team (factor_level_rows).  A
+    // a time (columns of a level are independent): a thin level a warp per
+    // column when it has at most one column per warp, else a thread per column,
+    // a fat one its block rows over the team (factor_level_rows).  A
     // non-SPD pivot only marks the scene, read once after the factorisation;
     // later columns then compute garbage in bounded loops.  Stands in for the
     // direct branch's SimplicialLDLT (:385-394).  Writes du; false on a non-SPD
@@ -2090,19 +2153,21 @@ class SceneSolver {
         if constexpr (kLargeTeam) return dense_solve_warp();
         Sparse S = sparse_ws();
         const int nlev = S.meta[0];
-        const int sub0 = S.sub_start[tid], sub1 = S.sub_start[tid + 1];
+        const int lane = tid & 31, w0 = tid - lane;
         int bad = 0;
         {  // each warp factors its lanes' subtrees, lane by lane, a warp per column
-            const int lane = tid & 31, w0 = tid - lane;
             for (int ln = 0; ln < 32; ++ln)
                 for (int q = S.sub_start[w0 + ln]; q < S.sub_start[w0 + ln + 1]; ++q)
                     bad |= factor_column_warp(S, S.sub_nodes[q], lane);
         }
         T.sync();
         for (int l = 0; l < nlev; ++l) {
+            const int lq0 = S.lvl_start[l], ncol = S.lvl_start[l + 1] - lq0;
             if (S.lvl_mode[l]) bad |= factor_level_rows(l);
-            else
-                for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) bad |= factor_column(S, S.lvl_nodes[q]);
+            else if (ncol <= (nt >> 5)) {  // few columns: a warp per column
+                if ((tid >> 5) < ncol) bad |= factor_column_warp(S, S.lvl_nodes[lq0 + (tid >> 5)], lane);
+            } else
+                for (int q = lq0 + tid; q < lq0 + ncol; q += nt) bad |= factor_column(S, S.lvl_nodes[q]);
             T.sync();  // level barrier; a failed pivot is checked once after the factorisation
         }
         {
@@ -2111,21 +2176,31 @@ class SceneSolver {
             bad = fl[0] > 0;
         }
         if (!bad) {
-            for (int q = sub0; q < sub1; ++q) forward_column(S, S.sub_nodes[q]);
+            for (int ln = 0; ln < 32; ++ln)
+                for (int q = S.sub_start[w0 + ln]; q < S.sub_start[w0 + ln + 1]; ++q)
+                    forward_column_warp(S, S.sub_nodes[q], lane);
             T.sync();
             for (int l = 0; l < nlev; ++l) {
+                const int lq0 = S.lvl_start[l], ncol = S.lvl_start[l + 1] - lq0;
                 if (S.lvl_mode[l]) forward_level_warp(l);
-                else
-                    for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) forward_column(S, S.lvl_nodes[q]);
+                else if (ncol <= (nt >> 5)) {
+                    if ((tid >> 5) < ncol) forward_column_warp(S, S.lvl_nodes[lq0 + (tid >> 5)], lane);
+                } else
+                    for (int q = lq0 + tid; q < lq0 + ncol; q += nt) forward_column(S, S.lvl_nodes[q]);
                 T.sync();
             }
             for (int l = nlev - 1; l >= 0; --l) {
+                const int lq0 = S.lvl_start[l], ncol = S.lvl_start[l + 1] - lq0;
                 if (S.lvl_mode[l]) backward_level_warp(l);
-                else
-                    for (int q = S.lvl_start[l] + tid; q < S.lvl_start[l + 1]; q += nt) backward_column(S, S.lvl_nodes[q]);
+                else if (ncol <= (nt >> 5)) {
+                    if ((tid >> 5) < ncol) backward_column_warp(S, S.lvl_nodes[lq0 + (tid >> 5)], lane);
+                } else
+                    for (int q = lq0 + tid; q < lq0 + ncol; q += nt) backward_column(S, S.lvl_nodes[q]);
                 T.sync();
             }
-            for (int q = sub1 - 1; q >= sub0; --q) backward_column(S, S.sub_nodes[q]);
+            for (int ln = 0; ln < 32; ++ln)
+                for (int q = S.sub_start[w0 + ln + 1] - 1; q >= S.sub_start[w0 + ln]; --q)
+                    backward_column_warp(S, S.sub_nodes[q], lane);
         }
         T.sync();
         return !bad;
