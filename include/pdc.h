@@ -243,24 +243,25 @@ int pdc_batch_solve_async(pdc_solver* s, const pdc_batch* batch,
 
 /* Allocation-free solve of one scene.  This entry point has no counterpart in
  * the reference.  It exists for callers that cannot allocate device memory while
- * stepping: a physics step recorded into a CUDA graph (cudaMalloc cannot be
- * captured), an engine that owns all device memory through its own pool or
- * budget, or a real-time loop that cannot afford an allocation's latency or
- * failure.  It needs no handle and calls no cudaMalloc/cudaFree: its scratch is
- * a fixed 12 MiB array inside the library (every GPU that loads the library holds
- * it until exit).  Every pointer in bodies/contacts/out is a DEVICE pointer the
+ * stepping: an engine that owns all device memory through its own pool or
+ * budget and does not let a library allocate behind it, or a real-time loop that
+ * cannot afford an allocation's latency, implicit synchronisation or failure.
+ * It needs no handle and calls no cudaMalloc/cudaFree: its scratch is a fixed
+ * 12 MiB array inside the library (every GPU that loads the library holds it
+ * until exit).  Every pointer in bodies/contacts/out is a DEVICE pointer the
  * caller owns (is_static and depth required); the work is enqueued on `stream`
  * (NULL = legacy default stream) on the calling thread's current device.
  * Limits: at most 256 bodies and 2048 contacts, else PDC_EINVAL; the sparse
- * factor's capacity (every pair of 256 bodies, 32,640 off-diagonal blocks) is the same as pdc_solve's, so a
- * scene inside the limits takes the same branch and gets the same results as
- * pdc_solve_async with warp teams off.  All calls share the scratch and it keeps
- * the last call's contents (the kernels reset what must start at zero), so calls
- * that overlap on the GPU race: serialise them.  Each call outside a stream
- * capture looks up the scratch's device address for the current device (so a
- * cudaDeviceReset between calls is harmless); a call made while `stream` is
- * capturing reuses the address found by the last uncaptured call on that device,
- * so make one call on each device before any capture.  `stats` (a DEVICE pointer
+ * factor's capacity (every pair of 256 bodies, 32,640 off-diagonal blocks) is
+ * the same as pdc_solve's, so a scene inside the limits takes the same branch
+ * and gets the same results as pdc_solve_async with warp teams off.  All calls
+ * share the scratch and it keeps the last call's contents (the kernels reset
+ * what must start at zero), so calls that overlap on the GPU race: serialise
+ * them.  Each call outside a stream capture looks up the scratch's device
+ * address for the current device (so a cudaDeviceReset between calls is
+ * harmless); a call made while `stream` is capturing reuses the address found
+ * by the last uncaptured call on that device.  The first call on a device does
+ * this set-up, so make it before any stream capture.  `stats` (a DEVICE pointer
  * to one pdc_stats, may be NULL) receives the solve's statistics and status;
  * out->stats is zeroed, not filled.  Errors are reported through
  * pdc_last_error(NULL). */

@@ -821,10 +821,11 @@ extern "C" void pdc_host_free(void* p) {
 // ---------------------------------------------------------------------------
 // Allocation-free single-scene solve.
 //
-// Some callers cannot allocate device memory at solve time: a physics step
-// recorded into a CUDA graph (cudaMalloc is not capturable), a host engine that
-// owns all device memory through its own pool or budget, or a real-time loop
-// where an allocation's latency or failure is not acceptable.  For them this
+// Some callers cannot allocate device memory at solve time: a host engine that
+// owns all device memory through its own pool or budget (and may not let a
+// library call cudaMalloc behind it), or a real-time loop where an
+// allocation's latency, its implicit synchronisation or its failure is not
+// acceptable.  For them this
 // entry point runs the same planner and solve kernels on a fixed scratch area
 // that lives in the library image itself (a file-scope __device__ array), so it
 // never calls cudaMalloc/cudaFree.  The caller still provides every input and
@@ -843,7 +844,8 @@ extern "C" void pdc_host_free(void* p) {
 // on it.  The array's device address is looked up (cudaGetSymbolAddress, with
 // the caller's device current) on every call whose stream is not capturing, so
 // it stays right after a cudaDeviceReset; a call on a capturing stream reuses
-// the address the last uncaptured call on that device found.
+// the address the last uncaptured call on that device found, so the first call
+// on each device (which does this set-up) must come before any stream capture.
 namespace {
 constexpr int kNoAllocMaxBodies = 256;
 constexpr int kNoAllocMaxContacts = 2048;

@@ -2,8 +2,9 @@
 existing device entry point pdc_solve_async on the same scene.
 
 pdc_solve_noalloc serves callers that cannot allocate device memory while
-stepping (a step captured in a CUDA graph, an engine with its own memory pool or
-budget, a real-time loop): it runs the same kernels on a fixed scratch array
+stepping (an engine that owns all device memory through its own pool or
+budget, a real-time loop that cannot afford an allocation's latency or
+failure): it runs the same kernels on a fixed scratch array
 inside the library.  The test buffers here are allocated by the test (torch);
 the entry point itself allocates nothing.  This file is collected last so a
 failure here does not hide any other test's result."""
