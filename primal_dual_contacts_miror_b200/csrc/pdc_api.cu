@@ -202,6 +202,9 @@ static size_t carve(Arena& A, int ns, long long nb, long long nc, pdc::BatchPtrs
     P->lam = D(2 * nc);
     P->fT = D(3 * nc);
     P->lT = D(2 * nc);
+    P->Xi2 = D(6 * nc);
+    P->fT2 = D(3 * nc);
+    P->lT2 = D(2 * nc);
     P->df = D(3 * nc);
     P->dl = D(2 * nc);
     P->rf = D(3 * nc);

@@ -137,7 +137,7 @@ struct CtaTeam {
     static constexpr int kind = 0;
     static constexpr int spmv_lanes = 1;  // lanes per body in the PCG product
     int rank, size, slot;
-    BlockReducer<8> red;
+    BlockReducer<16> red;
     int* s_int;  // shared: [0] carry, [1..32] warp partials
     __device__ CtaTeam(double* red_smem, int* int_smem) {
         rank = threadIdx.x;

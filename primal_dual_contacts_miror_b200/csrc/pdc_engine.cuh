@@ -116,6 +116,9 @@ struct BatchPtrs {
     double* lam;    // 2
     double* fT;     // 3
     double* lT;     // 2
+    double* Xi2;    // 6: the second line-search trial of a pair (Xi, fT, lT of step / 2)
+    double* fT2;    // 3
+    double* lT2;    // 2
     double* df;     // 3
     double* dl;     // 2
     double* rf;     // 3
@@ -317,9 +320,9 @@ class SceneSolver {
     // Gather sum over the incidences of body gb of sigma * [X; c x X]: the
     // contacts left sigma X in the body's own incidence slots (put_x), so the
     // loads are contiguous and independent of each other
-    __device__ __forceinline__ void gather(int gb, double out[6]) const {
+    __device__ __forceinline__ void gather(int gb, double out[6], const double* xbuf = nullptr) const {
         const int st = B.inc_start[gb], n = B.inc_cnt[gb];
-        const double* xi = B.Xi + 3LL * st;
+        const double* xi = (xbuf ? xbuf : B.Xi) + 3LL * st;
         const double* ai = B.armI + 3LL * st;
         double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
 #pragma unroll 4
@@ -334,10 +337,11 @@ class SceneSolver {
     }
     // Contact gc's world vector X into the incidence slots of its two sides, with
     // the side's sign (-X for side 0, X for side 1; static sides have no slot)
-    __device__ __forceinline__ void put_x(int gc, d3 x) const {
+    __device__ __forceinline__ void put_x(int gc, d3 x, double* xbuf = nullptr) const {
         const int s0 = B.islot[2 * gc], s1 = B.islot[2 * gc + 1];
-        if (s0 >= 0) st3(B.Xi + 3LL * s0, scl3(-1.0, x));
-        if (s1 >= 0) st3(B.Xi + 3LL * s1, x);
+        double* xo = xbuf ? xbuf : B.Xi;
+        if (s0 >= 0) st3(xo + 3LL * s0, scl3(-1.0, x));
+        if (s1 >= 0) st3(xo + 3LL * s1, x);
     }
     // (M / charMass) v  for an active body
     __device__ __forceinline__ void mass_mul(int gb, const double* v, double* y) const {
@@ -594,7 +598,7 @@ class SceneSolver {
     // weight, AC = max(f_n - (w_n + k + spring f_n), 0) - f_n; X = -R (f_n, 0, 0).
     __device__ __forceinline__ void normal_residual(int gc, const Frame& R, d3 w, double fn, double ln, double muc,
                                                     double* rfo, double* rlo, double& wrf2, double& rl2,
-                                                    double& ac2) const {
+                                                    double& ac2, double* xbuf = nullptr) const {
         double r0 = 0 - w.x;
         if (C.spring_based) r0 -= compliance * cm * fn;
         r0 += ln;
@@ -607,7 +611,7 @@ class SceneSolver {
         ac2 += a0 * a0;
         if (rfo) { rfo[0] = r0; rfo[1] = 0; rfo[2] = 0; }
         if (rlo) { rlo[0] = rl0; rlo[1] = 0; }
-        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, 0.0, 0.0})));
+        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, 0.0, 0.0})), xbuf);
     }
 
     // Residuals of one contact at the current iterate with its constraint values
@@ -655,11 +659,12 @@ class SceneSolver {
     }
 
     // ru = M(u - uold) (+ gather of T_j f); static rows zero (calculateResiduals :151-163)
-    __device__ __forceinline__ void body_residual(int gb, const double* ub, double* ru_out, double& ru2) const {
+    __device__ __forceinline__ void body_residual(int gb, const double* ub, double* ru_out, double& ru2,
+                                                  const double* xbuf = nullptr) const {
         double d[6], y[6], gth[6];
         for (int r = 0; r < 6; ++r) d[r] = ub[r] - B.uold[6 * gb + r];
         mass_mul(gb, d, y);
-        gather(gb, gth);
+        gather(gb, gth, xbuf);
         for (int r = 0; r < 6; ++r) {
             const double v = y[r] + gth[r];
             ru2 += v * v;
@@ -2743,69 +2748,129 @@ class SceneSolver {
         }
     }
 
+    // One contact of a line-search trial at `step` (filterLineSearch, the trial
+    // point f + 0.99 df, lambda + 0.99 dl, and its residuals): trial values into
+    // fo / lo, the world impulse into the incidence slots xbuf; adds |wrf|^2,
+    // |rl|^2, |AC|^2 to q[1..3] and the directional terms to q[5], q[6].
+    __device__ __forceinline__ void trial_contact(int gc, double step, double muc, double* fo, double* lo,
+                                                  double* xbuf, double* q) const {
+        double dfin[3], dlin[2], fI[3], lI[2];
+        filter(gc, step, dfin, dlin);
+        for (int k = 0; k < 2; ++k) lI[k] = __dadd_rn(B.lam[2 * gc + k], __dmul_rn(0.99, dlin[k]));
+        for (int k = 0; k < 3; ++k) fI[k] = __dadd_rn(B.f[3 * gc + k], __dmul_rn(0.99, dfin[k]));
+        for (int k = 0; k < 3; ++k) fo[3 * gc + k] = fI[k];
+        for (int k = 0; k < 2; ++k) lo[2 * gc + k] = lI[k];
+        // residual at the trial point u + 0.99 step du: J is linear, so its
+        // relative velocity is J u + 0.99 step J du (both stored per contact)
+        const Frame R = ld_frame(B.frame + 9 * gc);
+        const double a = __dmul_rn(0.99, step);
+        const d3 wu = ld3(B.wu + 3 * gc), wd = ld3(B.wd + 3 * gc);
+        const d3 w = d3{fma(a, wd.x, wu.x), fma(a, wd.y, wu.y), fma(a, wd.z, wu.z)};
+        double rfv[3], rlv[2];
+        contact_residual_w(gc, R, w, fI, lI, muc, rfv, rlv, q[1], q[2], q[3], xbuf);
+        q[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
+        q[6] += (dlin[0] / lI[0]) * rlv[0];
+        if (!C.only_normal) q[6] += (dlin[1] / lI[1]) * rlv[1];
+    }
+    // One active body of a line-search trial: |ru|^2 at u + 0.99 step du into
+    // q[0], du . ru into q[4]
+    __device__ __forceinline__ void trial_body(int gb, double step, const double* xbuf, double* q) const {
+        double ui[6], ruv[6];
+        trial_u(gb, step, ui);
+        double r2 = 0;
+        body_residual(gb, ui, ruv, r2, xbuf);
+        q[0] += r2;
+        for (int r = 0; r < 6; ++r) q[4] += (step * B.du[6 * gb + r]) * ruv[r];
+    }
+    // Acceptance of trial t (lineSearch :606-630): 1 = accept, 2 = stop without
+    // a step (the last trial failed), 0 = halve the step and go on.
+    __device__ __forceinline__ static int ls_verdict(const double* e, double sErr, double sacErr, int t, int maxLS) {
+        const double inErr = e[0] + e[1] + e[2];
+        const double sacIn = e[0] + e[3] + e[2];
+        const double gErr = -e[4] + e[5] + e[6];
+        const bool acpt = (inErr < sErr) | (sacIn < sacErr);
+        if ((acpt && gErr > 0) || (t == maxLS - 1)) return acpt ? 1 : 2;
+        return 0;
+    }
+    // Commit of an accepted trial at `step` with trial values fo / lo
+    __device__ __forceinline__ void ls_commit(double step, const double* fo, const double* lo) {
+        for (int i = tid; i < n_local; i += nt) {
+            const int gb = B.lbody[b0 + i];
+            if (!B.local[gb]) continue;
+            double ui[6];
+            trial_u(gb, step, ui);
+            for (int r = 0; r < 6; ++r) B.u[6 * gb + r] = ui[r];
+        }
+        for (int c = tid; c < nc; c += nt) {
+            const int gc = c0 + c;
+            for (int k = 0; k < 3; ++k) B.f[3 * gc + k] = fo[3 * gc + k];
+            for (int k = 0; k < 2; ++k) B.lam[2 * gc + k] = lo[2 * gc + k];
+        }
+        T.sync();
+    }
+
     // lineSearch (PrimalDualForceSolver.cpp:562-635).  Commits the accepted
     // trial into (u, f, lam) and returns the step (0 = nothing accepted).
+    // Thread-block teams with at most half a block of contacts and of local
+    // bodies evaluate trials in pairs (step and step / 2, one on each half of
+    // the block, the second with its own trial buffers): a contact or body sits
+    // at the same lane of the same warp position within its half as in a
+    // single trial, so every sum of the pair has the bits of the single
+    // trial's, and the trials and their verdicts are the sequential ones.
     __device__ double line_search(double sErr, double sacErr, double muc, int maxLS, int& trials) {
         double step = 1.0;
         trials = 0;
+        const int half = nt >> 1;
+        if constexpr (Team::kind == 0) {
+          if (nc <= half && n_local <= half) {
+            const int j = tid >= half ? 1 : 0, k = tid - j * half;
+            double* fo = j ? B.fT2 : B.fT;
+            double* lo = j ? B.lT2 : B.lT;
+            double* xo = j ? B.Xi2 : B.Xi;
+            for (int t = 0; t < maxLS; t += 2) {
+                const double sj = j ? step * 0.5 : step;
+                double q[7] = {0, 0, 0, 0, 0, 0, 0};
+                if (k < nc) trial_contact(c0 + k, sj, muc, fo, lo, xo, q);
+                T.sync();
+                if (k < n_local) {
+                    const int gb = B.lbody[b0 + k];
+                    if (active(gb)) trial_body(gb, sj, xo, q);
+                }
+                double e[14];
+#pragma unroll
+                for (int r = 0; r < 7; ++r) {
+                    e[r] = j ? 0.0 : q[r];
+                    e[7 + r] = j ? q[r] : 0.0;
+                }
+                T.sum(e);
+                ++trials;
+                int v = ls_verdict(e, sErr, sacErr, t, maxLS);
+                if (v == 1) { ls_commit(step, B.fT, B.lT); return step; }
+                if (v == 2) break;
+                if (t + 1 >= maxLS) break;
+                ++trials;
+                v = ls_verdict(e + 7, sErr, sacErr, t + 1, maxLS);
+                if (v == 1) { ls_commit(step * 0.5, B.fT2, B.lT2); return step * 0.5; }
+                if (v == 2) break;
+                step *= 0.25;
+            }
+            return 0.0;
+          }
+        }
         for (int t = 0; t < maxLS; ++t) {
             ++trials;
             double e[7] = {0, 0, 0, 0, 0, 0, 0};  // ru2, wrf2, rl2, ac2, du.ru, df.rf, (dl/l).rl
-            for (int c = tid; c < nc; c += nt) {
-                const int gc = c0 + c;
-                double dfin[3], dlin[2], fI[3], lI[2];
-                filter(gc, step, dfin, dlin);
-                for (int k = 0; k < 2; ++k) lI[k] = __dadd_rn(B.lam[2 * gc + k], __dmul_rn(0.99, dlin[k]));
-                for (int k = 0; k < 3; ++k) fI[k] = __dadd_rn(B.f[3 * gc + k], __dmul_rn(0.99, dfin[k]));
-                for (int k = 0; k < 3; ++k) B.fT[3 * gc + k] = fI[k];
-                for (int k = 0; k < 2; ++k) B.lT[2 * gc + k] = lI[k];
-                // residual at the trial point u + 0.99 step du: J is linear, so its
-                // relative velocity is J u + 0.99 step J du (both stored per contact)
-                const Frame R = ld_frame(B.frame + 9 * gc);
-                const double a = __dmul_rn(0.99, step);
-                const d3 wu = ld3(B.wu + 3 * gc), wd = ld3(B.wd + 3 * gc);
-                const d3 w = d3{fma(a, wd.x, wu.x), fma(a, wd.y, wu.y), fma(a, wd.z, wu.z)};
-                double rfv[3], rlv[2];
-                contact_residual_w(gc, R, w, fI, lI, muc, rfv, rlv, e[1], e[2], e[3]);
-                e[5] += dfin[0] * rfv[0] + dfin[1] * rfv[1] + dfin[2] * rfv[2];
-                e[6] += (dlin[0] / lI[0]) * rlv[0];
-                if (!C.only_normal) e[6] += (dlin[1] / lI[1]) * rlv[1];
-            }
+            for (int c = tid; c < nc; c += nt) trial_contact(c0 + c, step, muc, B.fT, B.lT, B.Xi, e);
             T.sync();
             for (int i = tid; i < n_local; i += nt) {
                 const int gb = B.lbody[b0 + i];
                 if (!active(gb)) continue;
-                double ui[6], ruv[6];
-                trial_u(gb, step, ui);
-                double r2 = 0;
-                body_residual(gb, ui, ruv, r2);
-                e[0] += r2;
-                for (int r = 0; r < 6; ++r) e[4] += (step * B.du[6 * gb + r]) * ruv[r];
+                trial_body(gb, step, B.Xi, e);
             }
             T.sum(e);
-            const double inErr = e[0] + e[1] + e[2];
-            const double sacIn = e[0] + e[3] + e[2];
-            const double gErr = -e[4] + e[5] + e[6];
-            const bool acpt = (inErr < sErr) | (sacIn < sacErr);
-            if ((acpt && gErr > 0) || (t == maxLS - 1)) {
-                if (acpt) {
-                    for (int i = tid; i < n_local; i += nt) {
-                        const int gb = B.lbody[b0 + i];
-                        if (!B.local[gb]) continue;
-                        double ui[6];
-                        trial_u(gb, step, ui);
-                        for (int r = 0; r < 6; ++r) B.u[6 * gb + r] = ui[r];
-                    }
-                    for (int c = tid; c < nc; c += nt) {
-                        const int gc = c0 + c;
-                        for (int k = 0; k < 3; ++k) B.f[3 * gc + k] = B.fT[3 * gc + k];
-                        for (int k = 0; k < 2; ++k) B.lam[2 * gc + k] = B.lT[2 * gc + k];
-                    }
-                    T.sync();
-                    return step;
-                }
-                break;
-            }
+            const int v = ls_verdict(e, sErr, sacErr, t, maxLS);
+            if (v == 1) { ls_commit(step, B.fT, B.lT); return step; }
+            if (v == 2) break;
             step *= 0.5;
         }
         return 0.0;
@@ -2817,9 +2882,9 @@ class SceneSolver {
     // contact residual with fresh constraints, given the relative velocity w
     __device__ __forceinline__ void contact_residual_w(int gc, const Frame& R, d3 w, const double* fv,
                                                        const double* lv, double muc, double* rfo, double* rlo,
-                                                       double& wrf2, double& rl2, double& ac2) const {
+                                                       double& wrf2, double& rl2, double& ac2, double* xbuf = nullptr) const {
         if (C.only_normal) {
-            normal_residual(gc, R, w, fv[0], lv[0], muc, rfo, rlo, wrf2, rl2, ac2);
+            normal_residual(gc, R, w, fv[0], lv[0], muc, rfo, rlo, wrf2, rl2, ac2, xbuf);
             return;
         }
         const double fn = fv[0], f1 = fv[1], f2 = fv[2];
@@ -2848,7 +2913,7 @@ class SceneSolver {
         ac2 += a0 * a0 + a1 * a1 + a2 * a2;
         rfo[0] = r0; rfo[1] = r1; rfo[2] = r2;
         rlo[0] = rl0; rlo[1] = rl1;
-        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})));
+        put_x(gc, scl3(-1.0, from_frame(R, d3{fn, f1, f2})), xbuf);
     }
 
     // KKT report at the final iterate (mu_c = 0) and write-back (:491-510).
@@ -3004,7 +3069,7 @@ __device__ __forceinline__ void run_scene(const BatchPtrs& B, const EngineCfg& C
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) solve_scenes_kernel(const __grid_constant__ BatchPtrs B,
                                                            const __grid_constant__ EngineCfg C) {
-    __shared__ double s_red[2 * 8 * 32];
+    __shared__ double s_red[2 * 16 * 32];
     __shared__ int s_int[33];
     __shared__ int s_q;
     {
