@@ -10,6 +10,9 @@ rest, in a walled column of footprint 10 sqrt(n/2000) m and height 40 m;
 mu 0.5, dt 0.01, g = (0, 0, -9.81)), FP64, Newton tolerance 1e-6.  The timed
 window is steps [settle + warmup, settle + warmup + steps) of the 500-step
 horizon; the working set (~3 GB) is larger than L2, so no flush is needed.
+Before the warm-up the autotuner (primal_dual_contacts_miror_b200/autotune.py)
+times the solve kernel's launch shapes on the world's current contact sets,
+untimed, and the world goes on with the fastest (--no-tune skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -45,12 +48,17 @@ sys.path.insert(0, ROOT)
 from primal_dual_contacts_miror_b200 import abi, scenes  # noqa: E402
 
 METRIC = "scene-steps/s"
+# launch shapes the autotuner times before the timed region: threads per block
+# of the batched solve kernel, and the contact / body limits of single-warp teams
+TUNE_SHAPES = [(256, 0, 0), (128, 0, 0), (256, 64, 32)]
 SEED = 20241203 + 3 * 10 ** 6  # the batched workload's seed
 DT = 0.01
 GRAVITY = (0.0, 0.0, -9.81)
-# DRAM bytes of one solve_scenes_kernel launch on this workload (ncu capture of
-# one launch at the middle of the timed window; profiles/)
-TRAFFIC_PER_LAUNCH = None
+# DRAM bytes of one solve_scenes_kernel launch on this workload: ncu's
+# dram__bytes of one launch on 1,024 box-drop scenes at world step 250 (31.5 GB;
+# the 4,096-scene world is above the capture size rule), scaled by the scene
+# count to a 4,096-scene launch (profiles/solve_scenes_kernel_boxdrops4096.md)
+TRAFFIC_PER_LAUNCH = 31.48e9 * 4
 
 
 def algorithmic_bytes(stats):
@@ -318,6 +326,26 @@ def run_headline(args, lib, torch, stream, local, rank, world):
     w.step(args.settle, sh)
     torch.cuda.synchronize()
     settle_s = time.perf_counter() - t0
+    tune = None
+    if not args.no_tune:
+        # the solve kernel's launch shape, picked by the autotuner on this
+        # world's current contact sets (untimed); the world is rebuilt with the
+        # winner from the same state
+        from primal_dual_contacts_miror_b200 import autotune
+
+        devb = lib.DeviceBatch(w.host_batch(), device=dev)
+        best, table = autotune.tune(devb, sys_cfg, torch, shapes=TUNE_SHAPES, warmup=1, steps=1, stream=stream)
+        del devb
+        key = lambda c: (c.cta_threads, c.warp_max_contacts, c.warp_max_bodies, c.pcg_lanes)
+        if key(best) != key(sys_cfg):
+            state = w.state()
+            w.close()
+            sys_cfg = best
+            w = lib.World(shapes, cfg=sys_cfg, contacts_per_body=16)
+            w.set_state(*state, stream=sh)
+            torch.cuda.synchronize()
+        tune = {"candidates": table, "chosen": dict(zip(("cta_threads", "warp_max_contacts", "warp_max_bodies",
+                                                          "pcg_lanes"), key(sys_cfg)))}
     w.step(args.warmup, sh)
     torch.cuda.synchronize()
     # per-step statistics of every scene, copied out after each timed step
@@ -376,7 +404,7 @@ def run_headline(args, lib, torch, stream, local, rank, world):
         "value": aggregate(args.scenes, world, ms_max / 1e3, args.steps), "ms_per_step": ms_max / args.steps,
         "clocks": clk, "kkt": kkt, "newton_iters_mean": newton, "contacts_per_step": contacts_per_step,
         "contact_newton_iters_per_s": ci * world / (ms_max / 1e3), "bodies_per_gpu": int(nb),
-        "untimed_settle_s": settle_s,
+        "untimed_settle_s": settle_s, "autotune": tune,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "host_memory": "page-locked (pdc_host_alloc)",
                 "api": "pdc_world_set_state + pdc_world_step + pdc_world_get_state, synchronized every step",
@@ -423,8 +451,9 @@ def run_world_legs(args, lib, torch, stream, local, rank, world, exported, cfg, 
     line["roofline"] = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": TRAFFIC_PER_LAUNCH, "peak_kind": peak_kind,
-        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one solve_scenes_kernel launch on "
-                          "this workload (profiles/)" if TRAFFIC_PER_LAUNCH else "not captured for this build",
+        "traffic_source": "ncu dram__bytes of one solve_scenes_kernel launch on 1,024 box-drop scenes at world "
+                          "step 250, scaled by the scene count to 4,096 (profiles/)" if TRAFFIC_PER_LAUNCH
+                          else "not captured for this build",
         "algorithmic_bytes_per_launch": float(np.mean(ab)), "launch_ms": float(np.mean(times)) * 1e3,
         "kernel": "solve_scenes_kernel (with its planner launch), on the world's next contact sets",
         "solve_share_of_step": float(np.mean(times)) * 1e3 / line["ms_per_step"],
@@ -647,6 +676,7 @@ def main():
     ap.add_argument("--pit-steps", type=int, default=200)
     ap.add_argument("--pile-steps", type=int, default=200)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--serve-rates", default="1000,5000,20000,50000")
     ap.add_argument("--serve-slots", type=int, default=2048)
     ap.add_argument("--serve-ticks", type=int, default=40)
@@ -681,7 +711,7 @@ def main():
         "newton_iters_mean": head["newton_iters_mean"], "kkt": head["kkt"],
         "contacts_per_step": head["contacts_per_step"], "bodies_per_gpu": head["bodies_per_gpu"],
         "contact_newton_iters_per_s": head["contact_newton_iters_per_s"],
-        "untimed_settle_s": head["untimed_settle_s"],
+        "untimed_settle_s": head["untimed_settle_s"], "autotune": head["autotune"],
     }
     cores = 0
     if rank == 0 and world == 1 and not args.no_cpu:
