@@ -628,6 +628,12 @@ def run_large(args, base_cfg, lib, torch, stream, cpu_cores):
             fc["cpu_cores"] = cpu_cores
             fc["cpu_oracle"] = {k: o[3][k] for k in ("status", "newton_iters", "pcg_iters")}
             fc["fp64_velocity_err_vs_oracle"] = err(g)
+            # the reference algorithm's own spread on this contact set: the
+            # oracle with the contacts in a permuted order
+            perm = np.random.default_rng(1).permutation(hs.n_contacts)
+            hp = abi.HostScene(hs.vel, hs.ang_vel, hs.mass, hs.inertia, hs.inv_inertia, hs.is_static,
+                               hs.body[perm], hs.frame[perm], hs.arm[perm], hs.depth[perm])
+            fc["oracle_vs_permuted_oracle"] = err(oracle_lib.solve(hp, dt=dt, cfg=cfg, nthreads=cpu_cores))
             fc["mixed_velocity_err_vs_oracle"] = err(m)
         out[name] = entry
     return out

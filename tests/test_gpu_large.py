@@ -71,17 +71,19 @@ _ORACLE = {}
 
 
 @pytest.mark.parametrize("team", sorted(TEAMS))
-@pytest.mark.parametrize("n_boxes,tol,bar", [(1500, 1e-8, 1e-6), (2100, 1e-6, 1e-4)])
+@pytest.mark.parametrize("n_boxes,tol,bar", [(1500, 1e-8, 1e-6), (2100, 1e-6, 1e-5)])
 def test_large_pile_matches_oracle(n_boxes, tol, bar, team):
     """1,500 boxes: direct branch (the large team's sparse block Cholesky on the
-    GPU, LDL^T in the oracle), Newton tolerance 1e-8.  2,100 boxes: iterative branch (block-Jacobi CG at
-    1e-8, cap 1000, on both sides) at the default Newton tolerance 1e-6; the
-    inexact CG directions trigger gradient-descent fall-backs on both sides, so
-    the bar there is a small multiple of the Newton tolerance.  The CG runs
-    must also stop where the reference's do: it solves the Jacobi-scaled
-    system D A D from the previous du as its scaled unknown and tests |D r| /
-    |D b|, so the total CG iteration count matches the oracle's within one per
-    Newton iteration (an unscaled start and test is 71 iterations off here)."""
+    GPU, LDL^T in the oracle), Newton tolerance 1e-8.  2,100 boxes: iterative
+    branch (block-Jacobi CG at 1e-8, cap 1000, on both sides) at the default
+    Newton tolerance 1e-6, velocities within 1e-5; the oracle against itself
+    with the contacts permuted moves them by ~1e-11 (measured: 4e-12 to 2e-11,
+    the same 16 Newton and 5,524 CG iterations), so the bar is the CG and
+    Newton tolerances' slack, not round-off.  The CG runs must also stop where
+    the reference's do: it solves the Jacobi-scaled system D A D from the
+    previous du as its scaled unknown and tests |D r| / |D b|, so the total CG
+    iteration count matches the oracle's within one per Newton iteration (an
+    unscaled start and test is 71 iterations off here)."""
     from primal_dual_contacts_miror_b200 import lib
 
     kind, cmax = TEAMS[team]
