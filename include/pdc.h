@@ -270,6 +270,32 @@ int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double gravity[3],
                       pdc_result* out, pdc_stats* stats, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Mesh bodies and mesh-mesh contacts (MeshMeshContactGenerator,
+ * src/Contact/ContactGenerator/MeshMeshContactGenerator.cpp:7-119, with
+ * Mesh::signedDistance, src/CollisionObject/Mesh.cpp:124-166).  A mesh is a
+ * closed, outward-oriented triangle surface in its body's frame; creation
+ * uploads it and builds the normals the signed distance needs (face, angle-
+ * weighted vertex and uniform edge normals, Mesh.cpp:56-63) on the calling
+ * thread's current device. */
+typedef struct pdc_mesh pdc_mesh;
+int pdc_mesh_create(int32_t n_verts, const double* verts /* [n][3] */, int32_t n_tris,
+                    const int32_t* tris /* [m][3] */, pdc_mesh** out);
+void pdc_mesh_destroy(pdc_mesh* m);
+/* Contact points of mesh bodies a (the lower body id) and b at poses
+ * (x, y, z, qx, qy, qz, qw): the vertices of every triangle of either mesh that
+ * overlaps a triangle of the other and lie inside the other mesh, with depth =
+ * -signed distance and the other mesh's vertex normals interpolated at the
+ * closest point as the normal (from a to b), then sorted and merged as
+ * DynamicSystem.cpp:343-381 merges a pair's points.  Host arrays: pos [3],
+ * normal [3], depth [1], frame [9] (row-major, normal in the first column) and
+ * arm [6] (pos - centre of a, pos - centre of b) per contact, at most
+ * max_points of them; *n_points = the number of contacts (more than max_points:
+ * only the first max_points written).  Synchronous. */
+int pdc_mesh_contacts(const pdc_mesh* a, const double pose_a[7], const pdc_mesh* b, const double pose_b[7],
+                      int32_t max_points, double* pos, double* normal, double* depth, double* frame,
+                      double* arm, int32_t* n_points);
+
+/* ------------------------------------------------------------------------
  * Device-resident time stepping (DynamicSystem::step, src/Dynamics/DynamicSystem.cpp:130-218,
  * fixed time step): contact detection (replacing FCL, DynamicSystem.cpp:219-227, with
  * analytic box/sphere/plane tests and the reference's post-processing, :247-383), the

@@ -959,4 +959,5 @@ extern "C" int pdc_solve_noalloc(const pdc_config* cfg, double dt, const double 
 }
 
 #include "pdc_world.cuh"
+#include "pdc_mesh.cuh"
 #include "pdc_server.cuh"

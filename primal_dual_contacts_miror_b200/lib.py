@@ -534,3 +534,65 @@ class DeviceBatch:
         raw = self.out_stats.cpu().numpy().tobytes()
         arr = (abi.Stats * self.n_scenes).from_buffer_copy(raw[: self.n_scenes * C.sizeof(abi.Stats)])
         return [s.as_dict() for s in arr]
+
+
+def _bind_mesh(lib):
+    if getattr(lib, "_mesh_bound", False):
+        return
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    lib.pdc_mesh_create.argtypes = [C.c_int32, dp, C.c_int32, ip, C.POINTER(C.c_void_p)]
+    lib.pdc_mesh_create.restype = C.c_int
+    lib.pdc_mesh_destroy.argtypes = [C.c_void_p]
+    lib.pdc_mesh_destroy.restype = None
+    lib.pdc_mesh_contacts.argtypes = [C.c_void_p, dp, C.c_void_p, dp, C.c_int32, dp, dp, dp, dp, dp, ip]
+    lib.pdc_mesh_contacts.restype = C.c_int
+    lib._mesh_bound = True
+
+
+class Mesh:
+    """A mesh body's surface on the device (pdc_mesh_create): vertices [n][3]
+    in the body frame, outward-oriented triangles [m][3]."""
+
+    def __init__(self, verts, tris):
+        self.lib = load()
+        _bind_mesh(self.lib)
+        self.V = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+        self.F = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 3)
+        h = C.c_void_p()
+        rc = self.lib.pdc_mesh_create(len(self.V), self.V.ctypes.data_as(C.POINTER(C.c_double)), len(self.F),
+                                      self.F.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(h))
+        if rc != abi.PDC_OK:
+            raise PdcError(rc, self.lib.pdc_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pdc_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mesh_contacts(a, pose_a, b, pose_b, max_points=4096):
+    """Contacts of mesh bodies a (the lower id) and b at poses (x, y, z, qx, qy,
+    qz, qw) (pdc_mesh_contacts): dict of pos [k][3], normal [k][3], depth [k],
+    frame [k][9], arm [k][6]."""
+    L = a.lib
+    pa = np.ascontiguousarray(pose_a, dtype=np.float64)
+    pb = np.ascontiguousarray(pose_b, dtype=np.float64)
+    out = {"pos": np.zeros((max_points, 3)), "normal": np.zeros((max_points, 3)), "depth": np.zeros(max_points),
+           "frame": np.zeros((max_points, 9)), "arm": np.zeros((max_points, 6))}
+    n = C.c_int32()
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    rc = L.pdc_mesh_contacts(a.h, dp(pa), b.h, dp(pb), max_points, dp(out["pos"]), dp(out["normal"]),
+                             dp(out["depth"]), dp(out["frame"]), dp(out["arm"]), C.byref(n))
+    if rc != abi.PDC_OK:
+        raise PdcError(rc, L.pdc_last_error(None).decode())
+    k = min(n.value, max_points)
+    res = {key: v[:k] for key, v in out.items()}
+    res["n"] = n.value
+    return res
