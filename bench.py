@@ -348,6 +348,12 @@ def run_headline(args, lib, torch, stream, local, rank, world):
                                                           "pcg_lanes"), key(sys_cfg)))}
     w.step(args.warmup, sh)
     torch.cuda.synchronize()
+    # the state at the start of the window: the end-to-end leg replays the same steps from it
+    nb = shapes.n
+    hpos, hquat, hvel, hang = (lib.pinned_empty((nb, 3)), lib.pinned_empty((nb, 4)), lib.pinned_empty((nb, 3)),
+                               lib.pinned_empty((nb, 3)))
+    w.get_state_async(hpos, hquat, hvel, hang, stream=sh)
+    torch.cuda.synchronize()
     # per-step statistics of every scene, copied out after each timed step
     ring = [lib.pinned_empty((C.sizeof(abi.Stats) * args.scenes,), np.uint8) for _ in range(args.steps)]
     ring_ptr = [C.cast(C.c_void_p(r.ctypes.data), C.POINTER(abi.Stats)) for r in ring]
@@ -373,14 +379,11 @@ def run_headline(args, lib, torch, stream, local, rank, world):
     contacts_per_step = float(np.sum([r.n_contacts for r in records])) / args.steps
     ci = float(np.sum([r.n_contacts * r.newton_iters for r in records]))
 
-    # end to end: the same steps driven from page-locked host state through the C ABI
-    nb = shapes.n
-    hpos, hquat, hvel, hang = (lib.pinned_empty((nb, 3)), lib.pinned_empty((nb, 4)), lib.pinned_empty((nb, 3)),
-                               lib.pinned_empty((nb, 3)))
+    # end to end: the same steps again, from the window's starting state (the
+    # solve is deterministic, so they repeat the device-timed steps), driven
+    # from page-locked host state through the C ABI
     hstats = lib.pinned_empty((C.sizeof(abi.Stats) * args.scenes,), np.uint8)
     hstats_p = C.cast(C.c_void_p(hstats.ctypes.data), C.POINTER(abi.Stats))
-    w.get_state_async(hpos, hquat, hvel, hang, stream=sh)
-    torch.cuda.synchronize()
     h2d = (3 + 4 + 3 + 3) * 8 * nb
     d2h = (3 + 4 + 3 + 3) * 8 * nb + C.sizeof(abi.Stats) * args.scenes
     barrier()
@@ -408,7 +411,7 @@ def run_headline(args, lib, torch, stream, local, rank, world):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "host_memory": "page-locked (pdc_host_alloc)",
                 "api": "pdc_world_set_state + pdc_world_step + pdc_world_get_state, synchronized every step",
-                "window": f"the {args.steps} steps after the device-timed window"},
+                "window": "the device-timed window's steps again, from its starting state"},
     }
     return head, exported, sys_cfg
 
