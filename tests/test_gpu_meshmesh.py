@@ -70,3 +70,29 @@ def test_mesh_contacts_truncate_and_reject_bad_meshes():
     with pytest.raises(lib.PdcError) as e:
         lib.Mesh(va, bad)
     assert e.value.code == abi.PDC_EINVAL
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_mesh_contacts_random_poses(seed):
+    """Seeded random overlapping poses of an icosphere against a box and of two
+    icospheres: the device equals the restatement to 1e-12."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    rng = np.random.default_rng(seed)
+    q = lambda: tuple(x / np.linalg.norm(x) for x in [rng.normal(size=4)])[0]
+    pairs = [(meshes.box((0.4, 0.3, 0.25)), meshes.icosphere(0.3, 2)),
+             (meshes.icosphere(0.35, 2), meshes.icosphere(0.25, 3))]
+    for (va, fa), (vb, fb) in pairs:
+        pa = (0.0, 0.0, 0.0) + tuple(q())
+        pb = tuple(rng.uniform(-0.25, 0.25, 3) + np.array([0.0, 0.0, 0.45])) + tuple(q())
+        ga, gb = lib.Mesh(va, fa), lib.Mesh(vb, fb)
+        got = lib.mesh_contacts(ga, pa, gb, pb)
+        ref = mm.contacts(mm.Mesh(va, fa), pa[:3], pa[3:], mm.Mesh(vb, fb), pb[:3], pb[3:])
+        assert got["n"] == len(ref), (seed, got["n"], len(ref))
+        for k, c in enumerate(ref):
+            np.testing.assert_allclose(got["pos"][k], c["pos"], atol=1e-12)
+            np.testing.assert_allclose(got["normal"][k], c["normal"], atol=1e-12)
+            np.testing.assert_allclose(got["depth"][k], c["depth"], atol=1e-12)
+            np.testing.assert_allclose(got["arm"][k], c["arm"], atol=1e-12)
+        ga.close()
+        gb.close()
