@@ -15,12 +15,19 @@ file or a list, relative to the YAML file), every mesh node of which becomes a
 box or sphere fitted to the mesh (primitives.py); bodies are numbered file by
 file, in the reference's type order (meshes, convex, cubes, ellipsoids,
 spheres), node order within a file; then `static:` and `initialize:` (id,
-density, velocity, angular_velocity) apply by body number.  Mesh, convex and
+density, velocity, angular_velocity) apply by body number.  Convex and
 ellipsoid bodies are not supported (the solver's narrow phase handles boxes,
 spheres and planes).  Bodies can also be given inline, numbered after the glTF
 ones: `boxes: [{half, pos, quat: [x, y, z, w], density}]`, `spheres: [{radius,
 pos, density}]`, `planes: [{point, normal: "+z"}]` (inline boxes and spheres
 default to density 1000, glTF ones to the reference's 1).
+
+`load_mesh_scene` reads a scene whose bodies are all `meshes:` (every mesh node
+of the named glTF files a mesh body, meshscene.mesh_body); `run` steps it as a
+meshscene.MeshScene.  Meshes in the same scene as cubes or spheres are
+rejected: the reference hands mesh-primitive pairs to FCL's own contact points
+(DynamicSystem.cpp:17-33: only mesh-mesh pairs get the mesh generator), which
+are not built here.
 """
 import os
 
@@ -118,6 +125,64 @@ def _gltf_files(node, key, base):
     return [os.path.join(base, n) for n in _entries(node, key) if isinstance(n, str)]
 
 
+def _base_dir(src, base_dir):
+    if base_dir is not None:
+        return base_dir
+    return os.path.dirname(os.path.abspath(src)) if isinstance(src, (str, os.PathLike)) else "."
+
+
+def is_mesh_scene(src):
+    """True when the scene's bodies are mesh bodies (`scene.meshes`)."""
+    node = _load(src).get("scene") or {}
+    return node.get("meshes") is not None
+
+
+def _init_entries(node):
+    init = {}
+    for o in (node.get("initialize") or []):
+        if "id" not in o:
+            raise ValueError("object_init: id is required")
+        init[int(o["id"])] = o
+    return init
+
+
+def load_mesh_scene(src, base_dir=None):
+    """Mesh bodies of a scene file's `scene:` section (FileLoader.cpp:42-111
+    with Mesh objects): one body per mesh node of each `meshes:` file, in file
+    and node order, then `static:` and `initialize:` by body number.  Returns
+    dict(bodies, warnings); every body a meshscene.mesh_body dict with vel,
+    ang_vel and is_static."""
+    from . import glb, meshscene
+
+    root = _load(src)
+    base_dir = _base_dir(src, base_dir)
+    node = root.get("scene") or {}
+    for key in ("convex", "ellipsoids"):
+        if node.get(key) is not None:
+            raise ValueError(f"scene.{key}: {key} bodies are not supported")
+    for key in ("cubes", "spheres", "boxes", "planes"):
+        if node.get(key) is not None:
+            raise ValueError(f"scene.{key}: meshes together with {key} are not supported (mesh-primitive pairs "
+                             "take FCL's contact points in the reference)")
+    nodes = [n for path in _gltf_files(node, "meshes", base_dir) for n in glb.read(path)]
+    if not nodes:
+        raise ValueError("scene: no bodies")
+    init = _init_entries(node)
+    static = {int(i) for i in (node.get("static") or [])}
+    warnings = [f"scene: {k} body id {i} out of range (0..{len(nodes) - 1}), ignored"
+                for k, ids in (("static", static), ("initialize", init)) for i in sorted(ids)
+                if not 0 <= i < len(nodes)]
+    bodies = []
+    for idx, n in enumerate(nodes):
+        o = init.get(idx, {})
+        b = meshscene.mesh_body(n["matrix"], n["positions"], n["triangles"], float(o.get("density", 1.0)))
+        b["vel"] = tuple(float(v) for v in o.get("velocity", (0, 0, 0)))
+        b["ang_vel"] = tuple(float(v) for v in o.get("angular_velocity", (0, 0, 0)))
+        b["is_static"] = idx in static
+        bodies.append(b)
+    return {"bodies": bodies, "warnings": warnings}
+
+
 def load_scene(src, base_dir=None):
     """Bodies of a scene file's `scene:` section as a shape-scene dict (the
     input of abi.ShapeBatch).  `base_dir`: where glTF names are resolved (the
@@ -125,10 +190,11 @@ def load_scene(src, base_dir=None):
     from . import glb, primitives
 
     root = _load(src)
-    if base_dir is None:
-        base_dir = os.path.dirname(os.path.abspath(src)) if isinstance(src, (str, os.PathLike)) else "."
+    base_dir = _base_dir(src, base_dir)
     node = root.get("scene") or {}
-    for key in ("meshes", "convex", "ellipsoids"):
+    if node.get("meshes") is not None:
+        raise ValueError("scene.meshes: a mesh scene (load_mesh_scene / meshscene.MeshScene), not a shape world")
+    for key in ("convex", "ellipsoids"):
         if node.get(key) is not None:
             raise ValueError(f"scene.{key}: {key} bodies are not supported (boxes, spheres and planes only)")
     rows = []  # (type, size, pos, quat, density)
@@ -147,11 +213,7 @@ def load_scene(src, base_dir=None):
     planes = list(node.get("planes") or [])
     if not rows and not planes:
         raise ValueError("scene: no bodies")
-    init = {}
-    for o in (node.get("initialize") or []):
-        if "id" not in o:
-            raise ValueError("object_init: id is required")
-        init[int(o["id"])] = o
+    init = _init_entries(node)
     static = {int(i) for i in (node.get("static") or [])}
     n_all = n_solid + len(planes)
     # The reference indexes its object list without a bounds check here
@@ -183,9 +245,18 @@ def run(scene_file, output_file, frames=None):
     sim = load_simulation(scene_file)
     if sim["backend"] != "gpu":
         raise ValueError("the device world runs the gpu backend only")
-    sc = load_scene(scene_file)
     dt = sim["timestep"]
     n = frames if frames is not None else frames_to_bake(sim["baking_time"], dt)
+    if is_mesh_scene(scene_file):
+        from . import meshscene
+
+        ms = meshscene.MeshScene(load_mesh_scene(scene_file)["bodies"], dt, sim["gravity"], cfg=sim["cfg"])
+        try:
+            return meshscene.bake(ms, n, output_file,
+                                  adaptive_factor=sim["substep_factor"] if sim["adaptive_timestep"] else None)
+        finally:
+            ms.close()
+    sc = load_scene(scene_file)
     w = lib.World(abi.ShapeBatch([sc], dt, sim["gravity"]), cfg=sim["cfg"])
     try:
         return filesaver.bake(w, 0, n, 1, output_file, dt,

@@ -1,0 +1,117 @@
+"""Mesh bodies and mesh scenes, host logic (no GPU): mesh-body mass properties
+as the reference builds them from a glTF node (RigidObjectBase.cpp:121-210,
+Mesh.cpp:18-123, FCL's BVH volume and inertia), the updateObjects
+integration of the mesh-scene stepper against the restatement's, the YAML
+scene path for `meshes:` (FileLoader.cpp:42-111) and the committed chain
+fixture (regenerated and compared when the reference checkout is present)."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from primal_dual_contacts_miror_b200 import meshes, meshscene, primitives, yamlcfg
+import mesh_fixture
+import world_ref
+
+REF = "/root/reference"
+
+
+def _rot(axis, ang):
+    a = np.asarray(axis, float) / np.linalg.norm(axis)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + math.sin(ang) * K + (1 - math.cos(ang)) * K @ K
+
+
+def test_box_mesh_body_mass_properties_and_pose():
+    v, f = meshes.box((0.5, 0.5, 0.5))
+    v = v + np.array([1.0, -2.0, 0.5])  # mesh centred away from its origin
+    R = _rot((1, 2, 3), 0.8)
+    s = np.array([0.4, 0.6, 1.0])  # the node stretches the unit cube to half extents 0.2, 0.3, 0.5
+    M = np.eye(4)
+    M[:3, :3] = R @ np.diag(s)
+    M[:3, 3] = (3.0, 4.0, 5.0)
+    b = meshscene.mesh_body(M, v, f, density=7.0)
+    h = 0.5 * s
+    vol = 8 * np.prod(h)
+    assert b["volume"] == pytest.approx(vol, rel=1e-12)
+    assert b["mass"] == pytest.approx(7.0 * vol, rel=1e-12)
+    m = b["mass"]
+    box_i = m / 3.0 * np.array([h[1] ** 2 + h[2] ** 2, h[0] ** 2 + h[2] ** 2, h[0] ** 2 + h[1] ** 2])
+    np.testing.assert_allclose(b["inertia0"], np.diag(box_i), atol=1e-12 * m)
+    # body position: the node translation plus the rotated, stretched mesh centre
+    np.testing.assert_allclose(b["pos"], M[:3, 3] + R @ (s * np.array([1.0, -2.0, 0.5])), atol=1e-12)
+    np.testing.assert_allclose(primitives.polar_decomposition(R)[0], R, atol=1e-12)
+    q = b["quat"]
+    np.testing.assert_allclose(world_ref.npr.quat_to_R(q), R, atol=1e-12)
+    np.testing.assert_allclose(b["verts"].mean(0), 0.0, atol=1e-12)  # centred on the centre of mass
+    assert meshscene.obb_min_length(b["verts"], b["tris"]) == pytest.approx(2 * h.min(), rel=1e-9)
+
+
+def test_icosphere_body_approaches_a_solid_sphere():
+    v, f = meshes.icosphere(0.3, 3)
+    b = meshscene.mesh_body(np.eye(4), v, f, density=1000.0)
+    sphere_m = 4 / 3 * math.pi * 0.3 ** 3 * 1000.0
+    assert b["mass"] == pytest.approx(sphere_m, rel=0.02)
+    np.testing.assert_allclose(np.diag(b["inertia0"]), 0.4 * b["mass"] * 0.3 ** 2, rtol=0.03)
+    off = b["inertia0"] - np.diag(np.diag(b["inertia0"]))
+    assert np.abs(off).max() < 1e-3 * b["inertia0"][0, 0]
+
+
+def test_integration_matches_restatement():
+    rng = np.random.default_rng(3)
+    n = 9
+    pos, vel, ang = rng.normal(size=(n, 3)), rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    quat = rng.normal(size=(n, 4))
+    quat /= np.linalg.norm(quat, axis=1, keepdims=True)
+    ang[4] = 0.0  # no rotation
+    dv, dw = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    static = np.zeros(n, bool)
+    static[[2, 7]] = True
+    a = [x.copy() for x in (pos, quat, vel, ang)]
+    b = [x.copy() for x in (pos, quat, vel, ang)]
+    meshscene.integrate(*a, dv, dw, static, 0.013)
+    world_ref.npr.integrate(*b, dv, dw, static, 0.013)
+    for x, y in zip(a, b):
+        np.testing.assert_allclose(x, y, atol=1e-15)
+
+
+def test_chain_fixture_through_the_yaml_path(tmp_path):
+    path = mesh_fixture.write_chain(str(tmp_path), links=4, yaml_edit=lambda t: t.replace(
+        "  static: [0]", "  static: [0, 9]\n  initialize:\n    - {id: 2, density: 3, velocity: [0, 1, 0]}"))
+    sc = yamlcfg.load_mesh_scene(path)
+    bodies = sc["bodies"]
+    assert len(bodies) == 4
+    assert [b["is_static"] for b in bodies] == [True, False, False, False]
+    assert sc["warnings"] == ["scene: static body id 9 out of range (0..3), ignored"]
+    assert bodies[2]["mass"] == pytest.approx(3 * bodies[1]["mass"])
+    assert bodies[2]["vel"] == (0.0, 1.0, 0.0)
+    s = 0.46818333864212036  # the links' glTF scale
+    for b in bodies:
+        # a torus of radii 1 and 0.25 scaled by s, as a polygon (12 x 48 here: within 5 %)
+        assert b["volume"] == pytest.approx(2 * math.pi ** 2 * 0.25 ** 2 * s ** 3, rel=0.05)
+        np.testing.assert_allclose(np.sqrt((b["spd"] ** 2).sum(0)), s, rtol=1e-6)
+        assert np.all(np.linalg.eigvalsh(b["inertia0"]) > 0)
+    # consecutive links hang 0.635 m apart along -y, turned a quarter turn about y
+    np.testing.assert_allclose([b["pos"][1] for b in bodies], [0.0, -0.6346, -1.2767, -1.9113], atol=2e-4)
+    sim = yamlcfg.load_simulation(path)
+    assert sim["adaptive_timestep"] and sim["substep_factor"] == 5.0
+    assert sim["cfg"].max_iter == 50 and sim["cfg"].tol == 1e-4 and sim["cfg"].mu == 0.6
+    assert tuple(sim["gravity"]) == (0.0, -9.81, 0.0)
+    assert yamlcfg.is_mesh_scene(path)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "scenes", "chain")), reason="reference checkout not present")
+def test_mesh_fixture_regenerates_from_reference_files():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "mk", os.path.join(os.path.dirname(mesh_fixture.FIXTURE), "make_mesh_scenes.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    d = np.load(mesh_fixture.FIXTURE)
+    for k, v in mk.load_chain(REF).items():
+        np.testing.assert_array_equal(np.asarray(v), d[k], err_msg=k)
+    # the full 128-link scene loads through the YAML path, link 0 static
+    sc = yamlcfg.load_mesh_scene(os.path.join(REF, "scenes", "chain", "chain.yaml"))
+    assert len(sc["bodies"]) == 128 and sc["bodies"][0]["is_static"] and not sc["bodies"][1]["is_static"]

@@ -92,6 +92,13 @@ def test_inline_scene_bodies():
 
 
 def test_unsupported_body_kinds_are_rejected_clearly():
-    for key in ("meshes", "convex", "ellipsoids"):
+    for key in ("convex", "ellipsoids"):
         with pytest.raises(ValueError, match="not supported"):
             yamlcfg.load_scene({"scene": {key: "bunny.glb"}})
+        with pytest.raises(ValueError, match="not supported"):
+            yamlcfg.load_mesh_scene({"scene": {"meshes": "chain.glb", key: "bunny.glb"}})
+    with pytest.raises(ValueError, match="mesh scene"):
+        yamlcfg.load_scene({"scene": {"meshes": "chain.glb"}})
+    for key in ("cubes", "spheres", "boxes", "planes"):
+        with pytest.raises(ValueError, match="meshes together with"):
+            yamlcfg.load_mesh_scene({"scene": {"meshes": "chain.glb", key: "floor.glb"}})

@@ -93,3 +93,79 @@ def step_adaptive(sc, state, T, gravity, cfg, factor):
 def initial_state(sc):
     return (np.array(sc["pos"], float).copy(), np.array(sc["quat"], float).copy(),
             np.array(sc["vel"], float).copy(), np.array(sc["ang_vel"], float).copy())
+
+
+# ---------------------------------------------------------------------------
+# Mesh scenes: numpy mesh-mesh contacts (oracle/meshmesh_ref.py) -> CPU oracle
+# solve -> numpy integration, with the adaptive substep rule on the world-space
+# vertex boxes.
+
+def mesh_models(bodies):
+    import meshmesh_ref as mm
+
+    return [mm.Mesh(b["verts"], b["tris"]) for b in bodies]
+
+
+def mesh_contact_scene(bodies, models, state):
+    """Every pair i < j (not both static) with the restatement's contacts, in
+    pair order; body state and world inertia as the solver takes them."""
+    import meshmesh_ref as mm
+
+    pos, quat, vel, ang = state
+    n = len(bodies)
+    W = [b["verts"] @ npr.quat_to_R(quat[k]).T + pos[k] for k, b in enumerate(bodies)]
+    lo, hi = [w.min(0) for w in W], [w.max(0) for w in W]
+    static = [bool(b.get("is_static", False)) for b in bodies]
+    rows = []
+    for i in range(n):
+        for j in range(i + 1, n):
+            if static[i] and static[j]:
+                continue
+            if not (np.all(lo[i] <= hi[j]) and np.all(lo[j] <= hi[i])):
+                continue  # boxes apart: no intersecting triangles
+            for c in mm.contacts(models[i], pos[i], quat[i], models[j], pos[j], quat[j]):
+                rows.append(((i, j), c))
+    inertia, inv_inertia = np.zeros((n, 6)), np.zeros((n, 6))
+    for k, b in enumerate(bodies):
+        R = npr.quat_to_R(quat[k])
+        i0 = np.asarray(b["inertia0"], float)
+        inertia[k] = sym6(R @ i0 @ R.T)
+        inv_inertia[k] = sym6(R @ np.linalg.inv(i0) @ R.T)
+    nc = len(rows)
+    hs = abi.HostScene(vel, ang, [b["mass"] for b in bodies], inertia, inv_inertia, static,
+                       np.array([r[0] for r in rows], np.int32).reshape(nc, 2),
+                       np.array([r[1]["frame"].reshape(-1) for r in rows]).reshape(nc, 9),
+                       np.array([r[1]["arm"] for r in rows]).reshape(nc, 6),
+                       np.array([r[1]["depth"] for r in rows]).reshape(nc))
+    return hs, rows
+
+
+def mesh_step(bodies, models, state, dt, gravity, cfg):
+    pos, quat, vel, ang = state
+    hs, rows = mesh_contact_scene(bodies, models, state)
+    dv, dw, lf, st = oracle_lib.solve(hs, dt=dt, gravity=gravity, cfg=cfg)
+    npr.integrate(pos, quat, vel, ang, dv, dw, [b.get("is_static", False) for b in bodies], dt)
+    return st, hs
+
+
+def mesh_substep(bodies, state, T, done, factor, min_length):
+    pos, quat, vel, ang = state
+    corners = []
+    for k, b in enumerate(bodies):
+        w = b["verts"] @ npr.quat_to_R(quat[k]).T + pos[k]
+        lo, hi = w.min(0), w.max(0)
+        c0, hs = 0.5 * (lo + hi), 0.5 * (hi - lo)
+        for c in range(8):
+            off = c0 + np.array([hs[0] if c & 4 else -hs[0], hs[1] if c & 2 else -hs[1],
+                                 hs[2] if c & 1 else -hs[2]]) - pos[k]
+            corners.append(vel[k] - np.cross(off, ang[k]))
+    corners = np.array(corners)
+    avg = 0.5 * (corners.min(0) + corners.max(0))
+    speed = np.sqrt(((corners - avg) ** 2).sum(1)).max()
+    return min(1.0 - done, min_length / (2 * (speed * T + 1e-8) * factor))
+
+
+def mesh_initial_state(bodies):
+    return (np.array([b["pos"] for b in bodies], float), np.array([b["quat"] for b in bodies], float),
+            np.array([b.get("vel", (0, 0, 0)) for b in bodies], float),
+            np.array([b.get("ang_vel", (0, 0, 0)) for b in bodies], float))
