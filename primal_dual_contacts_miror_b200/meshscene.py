@@ -35,7 +35,13 @@ import time as _time
 import numpy as np
 
 from . import abi, filesaver, primitives
-from .geometry import quat_to_matrix, sym6
+from .geometry import quat_to_matrix
+
+
+# AABB corner c has sign + on x when c & 4, on y when c & 2, on z when c & 1
+# (RigidObjectBase.cpp:89-93)
+_CORNER_SIGNS = np.array([[1.0 if c & 4 else -1.0, 1.0 if c & 2 else -1.0, 1.0 if c & 1 else -1.0]
+                          for c in range(8)])
 
 
 def _rotations(quat):
@@ -106,6 +112,33 @@ def integrate(pos, quat, vel, ang, dvel, dang, is_static, dt):
     quat[:, 3] = d * w - a * x - b * y - c * z
 
 
+def overlapping_pairs(lo, hi, is_static):
+    """Pairs (i < j) of boxes that overlap (closed boxes), not both static,
+    in lexicographic order."""
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    st = np.asarray(is_static, bool)
+    overlap = np.all(lo[:, None, :] <= hi[None, :, :], 2) & np.all(lo[None, :, :] <= hi[:, None, :], 2)
+    overlap &= ~(st[:, None] & st[None, :])
+    i, j = np.nonzero(np.triu(overlap, 1))  # row-major order
+    return list(zip(i.tolist(), j.tolist()))
+
+
+def substep_fraction(lo, hi, pos, vel, ang, min_length, dt, done, factor):
+    """Next substep as a fraction of the step dt (DynamicSystem.cpp:165-193):
+    the corner velocities of every body's box about the body's centre
+    (RigidObjectBase.cpp:86-105), their componentwise mid-range, the largest
+    speed about it, min_length / (2 (speed dt + 1e-8) factor), capped at what
+    is left of the step."""
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    centre, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    off = centre[:, None, :] + half[:, None, :] * _CORNER_SIGNS[None] - np.asarray(pos)[:, None, :]
+    corners = (np.asarray(vel)[:, None, :] - np.cross(off, np.asarray(ang)[:, None, :])).reshape(-1, 3)
+    avg = 0.5 * (corners.min(0) + corners.max(0))
+    speed = float(np.sqrt(((corners - avg) ** 2).sum(1)).max())
+    h = min_length / (2.0 * (speed * dt + 1e-8) * factor)
+    return min(1.0 - done, h)
+
+
 class MeshScene:
     """Mesh bodies of one scene, stepped on the GPU (contacts and solve) with
     host-side broad phase and integration.  `bodies`: dicts of mesh_body plus
@@ -156,18 +189,13 @@ class MeshScene:
     # -- one substep ------------------------------------------------------
     def pairs(self):
         """Body pairs (i < j, not both static) whose world vertex boxes overlap."""
+        lo, hi = self.boxes()
+        return overlapping_pairs(lo, hi, self.is_static)
+
+    def boxes(self):
+        """World-space vertex boxes (lo, hi) of every body."""
         W, _ = self.world_vertices()
-        lo = np.array([w.min(0) for w in W])
-        hi = np.array([w.max(0) for w in W])
-        out = []
-        n = len(W)
-        for i in range(n):
-            for j in range(i + 1, n):
-                if self.is_static[i] and self.is_static[j]:
-                    continue
-                if np.all(lo[i] <= hi[j]) and np.all(lo[j] <= hi[i]):
-                    out.append((i, j))
-        return out
+        return np.array([w.min(0) for w in W]), np.array([w.max(0) for w in W])
 
     def contact_scene(self):
         """The substep's contact problem (abi.HostScene) and the per-pair counts."""
@@ -187,8 +215,9 @@ class MeshScene:
                 depth.append(c["depth"])
             counts.append(((i, j), k))
         R = _rotations(self.quat)
-        inertia = np.array([sym6(R[k] @ self.i0[k] @ R[k].T) for k in range(len(R))])
-        inv_inertia = np.array([sym6(R[k] @ self.i0_inv[k] @ R[k].T) for k in range(len(R))])
+        sym = lambda m: np.stack([m[:, 0, 0], m[:, 1, 1], m[:, 2, 2], m[:, 0, 1], m[:, 0, 2], m[:, 1, 2]], 1)
+        inertia = sym(R @ self.i0 @ R.transpose(0, 2, 1))
+        inv_inertia = sym(R @ self.i0_inv @ R.transpose(0, 2, 1))
         cat = lambda xs, w: np.concatenate(xs) if xs else np.zeros((0, w))
         hs = abi.HostScene(self.vel, self.ang, self.mass, inertia, inv_inertia, self.is_static,
                            cat(body, 2).astype(np.int32), cat(frame, 9), cat(arm, 6),
@@ -211,20 +240,8 @@ class MeshScene:
     # -- adaptive substeps ------------------------------------------------
     def substep_fraction(self, done, factor):
         """Next substep as a fraction of the step (DynamicSystem.cpp:165-193)."""
-        W, _ = self.world_vertices()
-        corners = []
-        for k, w in enumerate(W):
-            lo, hi = w.min(0), w.max(0)
-            centre, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
-            for c in range(8):
-                sign = np.array([1.0 if c & 4 else -1.0, 1.0 if c & 2 else -1.0, 1.0 if c & 1 else -1.0])
-                off = centre + half * sign - self.pos[k]
-                corners.append(self.vel[k] - np.cross(off, self.ang[k]))
-        corners = np.array(corners)
-        avg = 0.5 * (corners.min(0) + corners.max(0))
-        speed = float(np.sqrt(((corners - avg) ** 2).sum(1)).max())
-        h = self.min_length / (2.0 * (speed * self.dt + 1e-8) * factor)
-        return min(1.0 - done, h)
+        lo, hi = self.boxes()
+        return substep_fraction(lo, hi, self.pos, self.vel, self.ang, self.min_length, self.dt, done, factor)
 
     def step_adaptive(self, n_steps, factor, max_substeps=100000):
         """Adaptive steps; returns the substep count of each step."""

@@ -115,3 +115,32 @@ def test_mesh_fixture_regenerates_from_reference_files():
     # the full 128-link scene loads through the YAML path, link 0 static
     sc = yamlcfg.load_mesh_scene(os.path.join(REF, "scenes", "chain", "chain.yaml"))
     assert len(sc["bodies"]) == 128 and sc["bodies"][0]["is_static"] and not sc["bodies"][1]["is_static"]
+
+
+def test_broad_phase_pairs_and_substep_rule_match_plain_loops():
+    rng = np.random.default_rng(5)
+    n = 12
+    centre = rng.uniform(-1, 1, (n, 3))
+    half = rng.uniform(0.05, 0.5, (n, 3))
+    lo, hi = centre - half, centre + half
+    lo[3], hi[3] = hi[2].copy(), hi[2] + 0.1  # boxes 2 and 3 touch at a face
+    static = np.zeros(n, bool)
+    static[[0, 5, 6]] = True
+    want = [(i, j) for i in range(n) for j in range(i + 1, n) if not (static[i] and static[j])
+            and np.all(lo[i] <= hi[j]) and np.all(lo[j] <= hi[i])]
+    assert meshscene.overlapping_pairs(lo, hi, static) == want
+    assert (2, 3) in want
+    # the substep rule against the host pipeline's statement (world_ref.mesh_substep)
+    bodies = []
+    for k in range(n):  # a body whose vertices are its box's corners, centre off the box centre
+        v = centre[k] + half[k] * np.array([[sx, sy, sz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)])
+        bodies.append({"verts": v - centre[k] + 0.3 * half[k], "tris": np.zeros((0, 3), np.int32)})
+    pos = centre - 0.3 * half
+    quat = np.tile([0.0, 0.0, 0.0, 1.0], (n, 1))
+    vel, ang = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    W = [b["verts"] + pos[k] for k, b in enumerate(bodies)]
+    blo, bhi = np.array([w.min(0) for w in W]), np.array([w.max(0) for w in W])
+    for done in (0.0, 0.6, 0.999):
+        got = meshscene.substep_fraction(blo, bhi, pos, vel, ang, 0.07, 0.01, done, 5.0)
+        ref = world_ref.mesh_substep(bodies, (pos, quat, vel, ang), 0.01, done, 5.0, 0.07)
+        assert got == pytest.approx(ref, rel=1e-14)
