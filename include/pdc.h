@@ -294,6 +294,18 @@ void pdc_mesh_destroy(pdc_mesh* m);
 int pdc_mesh_contacts(const pdc_mesh* a, const double pose_a[7], const pdc_mesh* b, const double pose_b[7],
                       int32_t max_points, double* pos, double* normal, double* depth, double* frame,
                       double* arm, int32_t* n_points);
+/* The contacts of n_pairs mesh pairs (a[k] the lower body id of pair k, poses
+ * [n_pairs][7]) in one call: the same points as pdc_mesh_contacts per pair,
+ * packed in pair order into the host arrays (at most max_points rows in all;
+ * counts[k] = pair k's contacts, *n_points = their sum, rows past max_points
+ * not written).  One set of device buffers per call and one copy of each
+ * output; DynamicSystem::generateContacts (src/Dynamics/DynamicSystem.cpp:
+ * 247-310) runs the pair generator over every FCL pair the same way.
+ * Synchronous. */
+int pdc_mesh_contacts_pairs(int32_t n_pairs, const pdc_mesh* const* a, const double* poses_a,
+                            const pdc_mesh* const* b, const double* poses_b, int32_t max_points, double* pos,
+                            double* normal, double* depth, double* frame, double* arm, int32_t* counts,
+                            int32_t* n_points);
 
 /* ------------------------------------------------------------------------
  * Device-resident time stepping (DynamicSystem::step, src/Dynamics/DynamicSystem.cpp:130-218,

@@ -261,6 +261,37 @@ __global__ void mesh_merge_kernel(int nva, int nvb, const int* inside, const dou
     *n_out = m;
 }
 
+// Pair k's merged contacts (rows of its own region, region k starting at row
+// row0[k]) copied to rows off_k .. off_k + n_k - 1 of the packed output, off_k
+// the sum of the counts of pairs 0 .. k-1, rows at or past `cap` dropped.
+__global__ void mesh_gather_kernel(int n_pairs, const int* counts, const long long* row0, const double* r_pos,
+                                   const double* r_nrm, const double* r_dep, const double* r_frame,
+                                   const double* r_arm, int cap, double* o_pos, double* o_nrm, double* o_dep,
+                                   double* o_frame, double* o_arm) {
+    __shared__ long long off;
+    const int k = blockIdx.x;
+    if (k >= n_pairs) return;
+    if (threadIdx.x == 0) {
+        long long o = 0;
+        for (int p = 0; p < k; ++p) o += counts[p];
+        off = o;
+    }
+    __syncthreads();
+    if (off >= cap) return;
+    const long long n = min((long long)counts[k], (long long)cap - off);
+    const long long src = row0[k];
+    for (long long r = threadIdx.x; r < n; r += blockDim.x) {
+        const long long a = src + r, d = off + r;
+        for (int c = 0; c < 3; ++c) {
+            o_pos[3 * d + c] = r_pos[3 * a + c];
+            o_nrm[3 * d + c] = r_nrm[3 * a + c];
+        }
+        o_dep[d] = r_dep[a];
+        for (int c = 0; c < 9; ++c) o_frame[9 * d + c] = r_frame[9 * a + c];
+        for (int c = 0; c < 6; ++c) o_arm[6 * d + c] = r_arm[6 * a + c];
+    }
+}
+
 }  // namespace pdc
 
 // ---------------------------------------------------------------------------
@@ -467,5 +498,111 @@ extern "C" int pdc_mesh_contacts(const pdc_mesh* a, const double pose_a[7], cons
         CK(cudaMemcpy(arm, o_arm, 6 * sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
     }
     *n_points = m;
+    return PDC_OK;
+}
+
+extern "C" int pdc_mesh_contacts_pairs(int32_t n_pairs, const pdc_mesh* const* a, const double* poses_a,
+                                       const pdc_mesh* const* b, const double* poses_b, int32_t max_points,
+                                       double* pos, double* normal, double* depth, double* frame, double* arm,
+                                       int32_t* counts, int32_t* n_points) {
+    pdc_solver* s = nullptr;
+    if (n_pairs < 0 || max_points < 0 || !n_points ||
+        (n_pairs > 0 && (!a || !b || !poses_a || !poses_b || !counts)) ||
+        (max_points > 0 && (!pos || !normal || !depth || !frame || !arm)))
+        return fail(s, PDC_EINVAL, "pdc_mesh_contacts_pairs: null or negative argument");
+    *n_points = 0;
+    if (n_pairs == 0) return PDC_OK;
+    for (int k = 0; k < n_pairs; ++k) {
+        if (!a[k] || !b[k]) return fail(s, PDC_EINVAL, "pdc_mesh_contacts_pairs: null mesh");
+        if (a[k]->device != a[0]->device || b[k]->device != a[0]->device)
+            return fail(s, PDC_EINVAL, "pdc_mesh_contacts_pairs: meshes on different devices");
+    }
+    CK(cudaSetDevice(a[0]->device), "cudaSetDevice");
+    // per-pair regions: ints (flags of a's and b's triangles, seeds and inside
+    // flags of both meshes' vertices), doubles (inside positions, normals and
+    // depths, then the merged rows), points (the merge's work array)
+    std::vector<long long> i0(n_pairs), d0(n_pairs), p0(n_pairs), row0(n_pairs);
+    long long ni = 0, nd = 0, np = 0, nrows = 0;
+    for (int k = 0; k < n_pairs; ++k) {
+        const long long nv = (long long)a[k]->nv + b[k]->nv;
+        i0[k] = ni; ni += (long long)a[k]->nf + b[k]->nf + 2 * nv;
+        d0[k] = nd; nd += 7 * nv;
+        p0[k] = np; np += nv;
+        row0[k] = nrows; nrows += nv;  // a pair merges at most its inside vertices
+    }
+    const long long cap = std::max<long long>(1, std::min<long long>(max_points, nrows));
+    DevScratch sc;
+    int *ibuf, *d_counts;
+    double *dbuf, *rows, *o_pos, *o_nrm, *o_dep, *o_frame, *o_arm;
+    long long* d_row0;
+    pdc::CPoint* pts;
+    cudaError_t e = sc.get(&ibuf, ni);
+    if (e == cudaSuccess) e = sc.get(&d_counts, n_pairs);
+    if (e == cudaSuccess) e = sc.get(&d_row0, n_pairs);
+    if (e == cudaSuccess) e = sc.get(&dbuf, nd);
+    if (e == cudaSuccess) e = sc.get(&rows, 22 * nrows);
+    if (e == cudaSuccess) e = sc.get(&pts, np);
+    if (e == cudaSuccess) e = sc.get(&o_pos, 22 * cap);
+    if (e != cudaSuccess) return cuda_fail(s, e, "pdc_mesh_contacts_pairs: scratch");
+    o_nrm = o_pos + 3 * cap; o_dep = o_nrm + 3 * cap; o_frame = o_dep + cap; o_arm = o_frame + 9 * cap;
+    double* r_pos = rows;
+    double* r_nrm = r_pos + 3 * nrows;
+    double* r_dep = r_nrm + 3 * nrows;
+    double* r_frame = r_dep + nrows;
+    double* r_arm = r_frame + 9 * nrows;
+    CK(cudaMemset(ibuf, 0, sizeof(int) * ni), "memset");
+    CK(cudaMemcpy(d_row0, row0.data(), sizeof(long long) * n_pairs, cudaMemcpyHostToDevice), "H2D rows");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, a[0]->device);
+    auto dev = [](const pdc_mesh* m, const double* pose) {
+        pdc::MeshDev d;
+        d.nv = m->nv; d.nf = m->nf;
+        d.V = m->V; d.F = m->F; d.fn = m->fn; d.vn = m->vn; d.en = m->en; d.emap = m->emap;
+        host_quat_to_R(pose + 3, d.R);
+        d.c = pdc::d3{pose[0], pose[1], pose[2]};
+        return d;
+    };
+    for (int k = 0; k < n_pairs; ++k) {  // the kernels of pdc_mesh_contacts, pair after pair on one stream
+        const pdc_mesh *ma = a[k], *mb = b[k];
+        const pdc::MeshDev A = dev(ma, poses_a + 7LL * k), B = dev(mb, poses_b + 7LL * k);
+        const int nv = ma->nv + mb->nv;
+        int* flag_a = ibuf + i0[k];
+        int* flag_b = flag_a + ma->nf;
+        int* seed = flag_b + mb->nf;
+        int* inside = seed + nv;
+        double* vpos = dbuf + d0[k];
+        double* vnrm = vpos + 3LL * nv;
+        double* vdep = vnrm + 3LL * nv;
+        const long long r = row0[k];
+        const long long pairs = (long long)ma->nf * mb->nf;
+        const int pblocks = (int)std::max(1LL, std::min<long long>((pairs + 255) / 256, 16LL * sms));
+        pdc::mesh_pairs_kernel<<<pblocks, 256>>>(A, B, flag_a, flag_b);
+        pdc::mesh_seed_kernel<<<std::max(1, std::min((ma->nf + 255) / 256, 8 * sms)), 256>>>(A, flag_a, seed);
+        pdc::mesh_seed_kernel<<<std::max(1, std::min((mb->nf + 255) / 256, 8 * sms)), 256>>>(B, flag_b,
+                                                                                           seed + ma->nv);
+        const int wblocks_a = std::max(1, std::min((ma->nv + 7) / 8, 16 * sms));
+        const int wblocks_b = std::max(1, std::min((mb->nv + 7) / 8, 16 * sms));
+        pdc::mesh_sdf_kernel<<<wblocks_a, 256>>>(A, B, seed, -1.0, inside, vpos, vnrm, vdep);
+        pdc::mesh_sdf_kernel<<<wblocks_b, 256>>>(B, A, seed + ma->nv, 1.0, inside + ma->nv, vpos + 3LL * ma->nv,
+                                                 vnrm + 3LL * ma->nv, vdep + ma->nv);
+        pdc::mesh_merge_kernel<<<1, 1>>>(ma->nv, mb->nv, inside, vpos, vnrm, vdep, pts + p0[k], A.c, B.c, nv,
+                                         r_pos + 3 * r, r_nrm + 3 * r, r_dep + r, r_frame + 9 * r, r_arm + 6 * r,
+                                         d_counts + k);
+    }
+    pdc::mesh_gather_kernel<<<n_pairs, 128>>>(n_pairs, d_counts, d_row0, r_pos, r_nrm, r_dep, r_frame, r_arm,
+                                              (int)cap, o_pos, o_nrm, o_dep, o_frame, o_arm);
+    CK(cudaGetLastError(), "launch mesh kernels");
+    CK(cudaMemcpy(counts, d_counts, sizeof(int32_t) * n_pairs, cudaMemcpyDeviceToHost), "D2H counts");
+    long long total = 0;
+    for (int k = 0; k < n_pairs; ++k) total += counts[k];
+    const long long w = std::min<long long>(total, max_points);
+    if (w > 0) {
+        CK(cudaMemcpy(pos, o_pos, 3 * sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
+        CK(cudaMemcpy(normal, o_nrm, 3 * sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
+        CK(cudaMemcpy(depth, o_dep, sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
+        CK(cudaMemcpy(frame, o_frame, 9 * sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
+        CK(cudaMemcpy(arm, o_arm, 6 * sizeof(double) * w, cudaMemcpyDeviceToHost), "D2H contacts");
+    }
+    *n_points = (int32_t)std::min<long long>(total, 0x7fffffffLL);
     return PDC_OK;
 }

@@ -546,6 +546,9 @@ def _bind_mesh(lib):
     lib.pdc_mesh_destroy.restype = None
     lib.pdc_mesh_contacts.argtypes = [C.c_void_p, dp, C.c_void_p, dp, C.c_int32, dp, dp, dp, dp, dp, ip]
     lib.pdc_mesh_contacts.restype = C.c_int
+    vp = C.POINTER(C.c_void_p)
+    lib.pdc_mesh_contacts_pairs.argtypes = [C.c_int32, vp, dp, vp, dp, C.c_int32, dp, dp, dp, dp, dp, ip, ip]
+    lib.pdc_mesh_contacts_pairs.restype = C.c_int
     lib._mesh_bound = True
 
 
@@ -595,4 +598,43 @@ def mesh_contacts(a, pose_a, b, pose_b, max_points=4096):
     k = min(n.value, max_points)
     res = {key: v[:k] for key, v in out.items()}
     res["n"] = n.value
+    return res
+
+
+def mesh_contact_buffers(max_points):
+    """Host output arrays for mesh_contacts_pairs (reusable across calls)."""
+    return {"pos": np.zeros((max_points, 3)), "normal": np.zeros((max_points, 3)), "depth": np.zeros(max_points),
+            "frame": np.zeros((max_points, 9)), "arm": np.zeros((max_points, 6))}
+
+
+def mesh_contacts_pairs(pairs, max_points=65536, out=None):
+    """Contacts of many mesh pairs in one call (pdc_mesh_contacts_pairs):
+    `pairs` = [(mesh a, pose a, mesh b, pose b)], a the lower body id.  Returns
+    dict of pos, normal, depth, frame, arm packed in pair order (views of
+    `out`, from mesh_contact_buffers(max_points), when given), counts (per
+    pair) and n (their sum; rows past max_points are not returned)."""
+    n_pairs = len(pairs)
+    if out is None:
+        out = mesh_contact_buffers(max_points)
+    max_points = min(len(out[k]) for k in ("pos", "normal", "depth", "frame", "arm"))
+    counts = np.zeros(max(n_pairs, 1), np.int32)
+    if n_pairs == 0:
+        res = {key: v[:0] for key, v in out.items()}
+        res["counts"], res["n"] = counts[:0], 0
+        return res
+    L = pairs[0][0].lib
+    ha = (C.c_void_p * n_pairs)(*[p[0].h.value for p in pairs])
+    hb = (C.c_void_p * n_pairs)(*[p[2].h.value for p in pairs])
+    pa = np.ascontiguousarray([p[1] for p in pairs], dtype=np.float64).reshape(n_pairs, 7)
+    pb = np.ascontiguousarray([p[3] for p in pairs], dtype=np.float64).reshape(n_pairs, 7)
+    n = C.c_int32()
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    rc = L.pdc_mesh_contacts_pairs(n_pairs, ha, dp(pa), hb, dp(pb), max_points, dp(out["pos"]), dp(out["normal"]),
+                                   dp(out["depth"]), dp(out["frame"]), dp(out["arm"]),
+                                   counts.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n))
+    if rc != abi.PDC_OK:
+        raise PdcError(rc, L.pdc_last_error(None).decode())
+    k = min(n.value, max_points)
+    res = {key: v[:k] for key, v in out.items()}
+    res["counts"], res["n"] = counts[:n_pairs], n.value
     return res

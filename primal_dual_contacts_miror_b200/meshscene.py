@@ -20,8 +20,9 @@ One substep on the GPU and host:
     static pairs skipped, pairs in (lower id, higher id) order as
     DynamicSystem.cpp:262-276 sorts them; a pair whose boxes are apart has no
     intersecting triangles, so this only prunes pairs;
-  * contacts (device): pdc_mesh_contacts per overlapping pair (triangle-pair
-    separating-axis seeds, signed distance, the pair merge);
+  * contacts (device): pdc_mesh_contacts_pairs over the overlapping pairs,
+    one call (triangle-pair separating-axis seeds, signed distance, the pair
+    merge, per pair);
   * solve (device): pdc_solve on the substep's contact set;
   * integration (host, a few hundred bodies at most in the reference's mesh
     scenes): updateObjects (DynamicSystem.cpp:137-161).
@@ -144,7 +145,7 @@ class MeshScene:
     host-side broad phase and integration.  `bodies`: dicts of mesh_body plus
     optional vel, ang_vel, is_static."""
 
-    def __init__(self, bodies, dt, gravity, cfg=None, max_points_per_pair=8192):
+    def __init__(self, bodies, dt, gravity, cfg=None, max_points=65536):
         from . import lib
 
         if not bodies:
@@ -153,7 +154,8 @@ class MeshScene:
         self.dt = float(dt)
         self.gravity = tuple(float(g) for g in gravity)
         self.cfg = cfg if cfg is not None else abi.default_config()
-        self.max_points = int(max_points_per_pair)
+        self.max_points = int(max_points)
+        self.buffers = lib.mesh_contact_buffers(self.max_points)
         self.bodies = bodies
         self.meshes = [lib.Mesh(b["verts"], b["tris"]) for b in bodies]
         self.solver = lib.Solver(self.cfg)
@@ -198,30 +200,22 @@ class MeshScene:
         return np.array([w.min(0) for w in W]), np.array([w.max(0) for w in W])
 
     def contact_scene(self):
-        """The substep's contact problem (abi.HostScene) and the per-pair counts."""
-        body, frame, arm, depth, counts = [], [], [], [], []
-        for i, j in self.pairs():
-            pa = np.concatenate([self.pos[i], self.quat[i]])
-            pb = np.concatenate([self.pos[j], self.quat[j]])
-            c = self.lib.mesh_contacts(self.meshes[i], pa, self.meshes[j], pb, self.max_points)
-            if c["n"] > self.max_points:
-                raise RuntimeError(f"bodies {i}, {j}: {c['n']} contact points, more than max_points_per_pair "
-                                   f"= {self.max_points}")
-            k = c["n"]
-            if k:
-                body.append(np.tile(np.array([i, j], np.int32), (k, 1)))
-                frame.append(c["frame"])
-                arm.append(c["arm"])
-                depth.append(c["depth"])
-            counts.append(((i, j), k))
+        """The substep's contact problem (abi.HostScene) and the per-pair counts:
+        every overlapping pair's contacts from one pdc_mesh_contacts_pairs call."""
+        pairs = self.pairs()
+        pose = np.concatenate([self.pos, self.quat], 1)
+        c = self.lib.mesh_contacts_pairs([(self.meshes[i], pose[i], self.meshes[j], pose[j]) for i, j in pairs],
+                                         out=self.buffers)
+        if c["n"] > self.max_points:
+            raise RuntimeError(f"{c['n']} contact points, more than max_points = {self.max_points}")
+        body = np.repeat(np.array(pairs, np.int32).reshape(-1, 2), c["counts"], axis=0)
+        counts = list(zip(pairs, c["counts"].tolist()))
         R = _rotations(self.quat)
         sym = lambda m: np.stack([m[:, 0, 0], m[:, 1, 1], m[:, 2, 2], m[:, 0, 1], m[:, 0, 2], m[:, 1, 2]], 1)
         inertia = sym(R @ self.i0 @ R.transpose(0, 2, 1))
         inv_inertia = sym(R @ self.i0_inv @ R.transpose(0, 2, 1))
-        cat = lambda xs, w: np.concatenate(xs) if xs else np.zeros((0, w))
         hs = abi.HostScene(self.vel, self.ang, self.mass, inertia, inv_inertia, self.is_static,
-                           cat(body, 2).astype(np.int32), cat(frame, 9), cat(arm, 6),
-                           np.concatenate(depth) if depth else np.zeros(0))
+                           body, c["frame"].copy(), c["arm"].copy(), c["depth"].copy())  # off the reused buffers
         return hs, counts
 
     def substep(self, h):

@@ -96,3 +96,33 @@ def test_mesh_contacts_random_poses(seed):
             np.testing.assert_allclose(got["arm"][k], c["arm"], atol=1e-12)
         ga.close()
         gb.close()
+
+
+def test_mesh_contacts_pairs_equal_one_call_per_pair():
+    """pdc_mesh_contacts_pairs packs, in pair order, bitwise the points that
+    pdc_mesh_contacts returns pair by pair (a separated pair included), and
+    truncates at max_points with the full counts."""
+    from primal_dual_contacts_miror_b200 import lib
+
+    made, pairs = [], []
+    for name in sorted(CASES):
+        (va, fa), pa, (vb, fb), pb = CASES[name]
+        ga, gb = lib.Mesh(va, fa), lib.Mesh(vb, fb)
+        made += [ga, gb]
+        pairs.append((ga, pa, gb, pb))
+    pairs.append(pairs[0])  # the same meshes twice in one call
+    singles = [lib.mesh_contacts(a, pa, b, pb) for a, pa, b, pb in pairs]
+    got = lib.mesh_contacts_pairs(pairs)
+    assert list(got["counts"]) == [s["n"] for s in singles]
+    assert got["n"] == sum(s["n"] for s in singles) and 0 in got["counts"]
+    for k in ("pos", "normal", "depth", "frame", "arm"):
+        np.testing.assert_array_equal(got[k], np.concatenate([s[k] for s in singles]), err_msg=k)
+    cut = got["n"] - 3
+    part = lib.mesh_contacts_pairs(pairs, max_points=cut)
+    assert part["n"] == got["n"] and list(part["counts"]) == list(got["counts"])
+    for k in ("pos", "normal", "depth", "frame", "arm"):
+        np.testing.assert_array_equal(part[k], got[k][:cut], err_msg=k)
+    none = lib.mesh_contacts_pairs([])
+    assert none["n"] == 0 and len(none["pos"]) == 0
+    for m in made:
+        m.close()
