@@ -134,15 +134,33 @@ def square_mesh():
 def write_gltf(path, types, sizes, pos, quat):
     """The scene file: per body a mesh of its collision geometry and a node with
     the total transform [R diag(scale) | p]; buffers in `<base>.bin`."""
-    import json
-
-    base = os.path.splitext(path)[0]
     meshes = {abi.PDC_SHAPE_BOX: cube_mesh(), abi.PDC_SHAPE_SPHERE: icosphere_mesh(3),
               abi.PDC_SHAPE_PLANE: square_mesh()}
     R = quat_to_matrix(np.asarray(quat, np.float64).reshape(-1, 4))
-    blob, views, accessors, gmeshes, nodes = bytearray(), [], [], [], []
+    body_meshes, matrices = [], []
     for i, t in enumerate(types):
-        v, f = meshes[int(t)]
+        body_meshes.append(meshes[int(t)])
+        scale = render_scale(int(t), sizes[i])
+        if int(t) == abi.PDC_SHAPE_PLANE:
+            scale = np.full(3, 100.0)
+        M = np.eye(4)
+        M[:3, :3] = R[i] * scale[None, :]
+        M[:3, 3] = pos[i]
+        matrices.append(M)
+    return write_gltf_meshes(path, body_meshes, matrices)
+
+
+def write_gltf_meshes(path, body_meshes, matrices):
+    """A .gltf scene (+ `<base>.bin`) with mesh `mesh_<i>` = body_meshes[i]
+    (vertices [n][3], triangles [m][3], stored as float32 / uint32) under a
+    top-level node of 4x4 transform matrices[i] (FileSaver.cpp:44-137)."""
+    import json
+
+    base = os.path.splitext(path)[0]
+    blob, views, accessors, gmeshes, nodes = bytearray(), [], [], [], []
+    for i, (v, f) in enumerate(body_meshes):
+        v = np.asarray(v, np.float32).reshape(-1, 3)
+        f = np.asarray(f, np.uint32).reshape(-1, 3)
         for arr, target, ctype, kind in ((v, 34962, 5126, "VEC3"), (f.reshape(-1), 34963, 5125, "SCALAR")):
             raw = arr.astype(arr.dtype.newbyteorder("<")).tobytes()
             views.append({"buffer": 0, "byteOffset": len(blob), "byteLength": len(raw), "target": target})
@@ -154,21 +172,16 @@ def write_gltf(path, types, sizes, pos, quat):
             blob += raw + b"\0" * (-len(raw) % 4)
         gmeshes.append({"name": f"mesh_{i}", "primitives": [
             {"attributes": {"POSITION": len(accessors) - 2}, "indices": len(accessors) - 1, "mode": 4}]})
-        scale = render_scale(int(t), sizes[i])
-        if int(t) == abi.PDC_SHAPE_PLANE:
-            scale = np.full(3, 100.0)
-        M = np.eye(4)
-        M[:3, :3] = R[i] * scale[None, :]
-        M[:3, 3] = pos[i]
+        M = np.asarray(matrices[i], np.float64)
         nodes.append({"name": str(i), "mesh": i, "matrix": [float(x) for x in M.T.reshape(-1)]})
     doc = {"asset": {"version": "2.0", "generator": "primal_dual_contacts_miror_b200.filesaver"},
            "buffers": [{"uri": os.path.basename(base) + ".bin", "byteLength": len(blob)}],
            "bufferViews": views, "accessors": accessors, "meshes": gmeshes, "nodes": nodes,
            "scenes": [{"name": "scene", "nodes": list(range(len(nodes)))}], "scene": 0}
-    with open(base + ".bin", "wb") as f:
-        f.write(bytes(blob))
-    with open(base + ".gltf", "w") as f:
-        json.dump(doc, f)
+    with open(base + ".bin", "wb") as fh:
+        fh.write(bytes(blob))
+    with open(base + ".gltf", "w") as fh:
+        json.dump(doc, fh)
     return base + ".gltf"
 
 

@@ -51,8 +51,9 @@ def _rotations(quat):
 
 def mesh_body(matrix, positions, triangles, density=1.0):
     """A mesh body from a node transform and its mesh: dict(verts (centred,
-    body frame), tris, pos, quat, mass, inertia0 (3x3 body frame, at
-    `density`), volume, inertia_unit (unit density), spd, com)."""
+    body frame), tris, positions (the mesh's own vertices), pos, quat, mass,
+    inertia0 (3x3 body frame, at `density`), volume, inertia_unit (unit
+    density), spd, com)."""
     M = np.asarray(matrix, np.float64)
     tris = np.asarray(triangles, np.int64).reshape(-1, 3)
     rot, spd = primitives.polar_decomposition(M[:3, :3])
@@ -65,7 +66,8 @@ def mesh_body(matrix, positions, triangles, density=1.0):
     J = J + volume * np.array([[-(y * y + z * z), x * y, x * z],
                                [y * x, -(x * x + z * z), y * z],
                                [z * x, z * y, -(x * x + y * y)]])
-    return {"verts": verts, "tris": tris.astype(np.int32), "pos": M[:3, 3] + rot @ com,
+    return {"verts": verts, "tris": tris.astype(np.int32), "positions": np.asarray(positions, np.float64),
+            "pos": M[:3, 3] + rot @ com,
             "quat": primitives.rot_to_quat(rot), "volume": volume, "inertia_unit": J,
             "mass": volume * density, "inertia0": J * density, "spd": spd, "com": com}
 
@@ -273,11 +275,26 @@ def saved_rows(bodies, pos, quat):
     return rows
 
 
+def total_transforms(bodies, pos, quat):
+    """Each body's mesh-to-world transform [R S | pos - R c] (the rigid pose
+    times the permanent stretch, RigidObjectBase's getTotalTransMatrix)."""
+    R = _rotations(quat)
+    out = []
+    for k, b in enumerate(bodies):
+        M = np.eye(4)
+        M[:3, :3] = R[k] @ b["spd"]
+        M[:3, 3] = pos[k] - R[k] @ b["com"]
+        out.append(M)
+    return out
+
+
 def bake(scene, frames, path, adaptive_factor=None):
     """The CLI's baking loop (SimulationSceneCLI.cpp:9-20) on a MeshScene:
     `frames` steps, one saved frame after each, then `<path>.npz` (scale row =
-    the column lengths of each body's stretch, then the frames) and
-    `<path>.info`.  Returns the two file names."""
+    the column lengths of each body's stretch, then the frames), `<path>.info`
+    and the scene `<path>.gltf` (+ `.bin`: each body's own mesh under its total
+    transform at the last frame, FileSaver.cpp:44-137).  Returns the .npz and
+    .info names."""
     base = os.path.splitext(path)[0]
     frames_out, times = [], []
     t, wall, contacts, substeps = 0.0, 0.0, 0, 0
@@ -301,6 +318,8 @@ def bake(scene, frames, path, adaptive_factor=None):
             a[f + 1] = rows[k]
         arrays[f"mesh_{k}"] = a
     np.savez(base + ".npz", **arrays)
+    filesaver.write_gltf_meshes(base + ".gltf", [(b["positions"], b["tris"]) for b in scene.bodies],
+                                total_transforms(scene.bodies, scene.pos, scene.quat))
     st = scene.last_stats or {}
     n = max(frames, 1)
     with open(base + ".info", "w") as f:

@@ -75,6 +75,13 @@ def test_mesh_scene_bake_writes_the_reference_layout(tmp_path):
     np.testing.assert_allclose(d["mesh_0"][1:, :3], 0.0, atol=1e-8)  # the static link stays put
     assert d["mesh_1"][3, 1] < d["mesh_1"][1, 1]  # the next one falls
     assert "Total #solids: 3" in open(info).read()
+    import json
+
+    doc = json.load(open(tmp_path / "out.gltf"))  # each link's own mesh under its total transform
+    assert [m["name"] for m in doc["meshes"]] == ["mesh_0", "mesh_1", "mesh_2"]
+    assert doc["accessors"][0]["count"] == 637 and doc["accessors"][1]["count"] == 3 * 1152
+    T = np.array(doc["nodes"][1]["matrix"]).reshape(4, 4).T
+    np.testing.assert_allclose(T[:3, 3], d["mesh_1"][3, :3], atol=1e-12)  # the last saved frame
 
 
 def test_box_and_sphere_meshes_on_a_floor_match_host_pipeline():

@@ -144,3 +144,24 @@ def test_broad_phase_pairs_and_substep_rule_match_plain_loops():
         got = meshscene.substep_fraction(blo, bhi, pos, vel, ang, 0.07, 0.01, done, 5.0)
         ref = world_ref.mesh_substep(bodies, (pos, quat, vel, ang), 0.01, done, 5.0, 0.07)
         assert got == pytest.approx(ref, rel=1e-14)
+
+
+def test_total_transform_maps_the_mesh_to_its_world_vertices():
+    """The .gltf node of a mesh body (its own mesh under the total transform)
+    lands on the body's world-space collision vertices."""
+    v, f = meshes.icosphere(0.4, 1)
+    v = v + np.array([0.3, -0.2, 0.1])
+    M = np.eye(4)
+    M[:3, :3] = _rot((0, 1, 1), 0.5) @ np.diag([1.0, 0.5, 2.0]) @ _rot((1, 0, 0), 0.3).T
+    M[:3, 3] = (1.0, 2.0, 3.0)
+    b = meshscene.mesh_body(M, v, f)
+    rng = np.random.default_rng(8)
+    pos = rng.normal(size=(1, 3))
+    quat = rng.normal(size=(1, 4))
+    quat /= np.linalg.norm(quat)
+    T = meshscene.total_transforms([b], pos, quat)[0]
+    world = v @ T[:3, :3].T + T[:3, 3]
+    R = world_ref.npr.quat_to_R(quat[0])
+    np.testing.assert_allclose(world, b["verts"] @ R.T + pos[0], atol=1e-12)
+    # at the initial pose the total transform is the node's own matrix
+    np.testing.assert_allclose(meshscene.total_transforms([b], [b["pos"]], [b["quat"]])[0], M, atol=1e-12)
