@@ -117,13 +117,24 @@ def integrate(pos, quat, vel, ang, dvel, dang, is_static, dt):
 
 def overlapping_pairs(lo, hi, is_static):
     """Pairs (i < j) of boxes that overlap (closed boxes), not both static,
-    in lexicographic order."""
-    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
-    st = np.asarray(is_static, bool)
-    overlap = np.all(lo[:, None, :] <= hi[None, :, :], 2) & np.all(lo[None, :, :] <= hi[:, None, :], 2)
-    overlap &= ~(st[:, None] & st[None, :])
-    i, j = np.nonzero(np.triu(overlap, 1))  # row-major order
-    return list(zip(i.tolist(), j.tolist()))
+    in lexicographic order.  Sweep and prune on x: boxes sorted by lo.x, each
+    paired with the later boxes whose lo.x is at most its hi.x (those overlap
+    it on x), then tested on y and z."""
+    lo, hi = np.asarray(lo, np.float64).reshape(-1, 3), np.asarray(hi, np.float64).reshape(-1, 3)
+    st = np.asarray(is_static, bool).reshape(-1)
+    n = len(lo)
+    order = np.argsort(lo[:, 0], kind="stable")
+    slo = lo[order, 0]
+    end = np.searchsorted(slo, hi[order, 0], side="right")  # first sorted box starting past hi.x
+    cnt = np.maximum(end - np.arange(1, n + 1), 0)
+    p = np.repeat(np.arange(n), cnt)
+    q = np.arange(cnt.sum()) - np.repeat(np.cumsum(cnt) - cnt, cnt) + p + 1
+    a, b = order[p], order[q]
+    i, j = np.minimum(a, b), np.maximum(a, b)
+    keep = np.all(lo[i, 1:] <= hi[j, 1:], 1) & np.all(lo[j, 1:] <= hi[i, 1:], 1) & ~(st[i] & st[j])
+    i, j = i[keep], j[keep]
+    o = np.lexsort((j, i))
+    return list(zip(i[o].tolist(), j[o].tolist()))
 
 
 def substep_fraction(lo, hi, pos, vel, ang, min_length, dt, done, factor):

@@ -165,3 +165,17 @@ def test_total_transform_maps_the_mesh_to_its_world_vertices():
     np.testing.assert_allclose(world, b["verts"] @ R.T + pos[0], atol=1e-12)
     # at the initial pose the total transform is the node's own matrix
     np.testing.assert_allclose(meshscene.total_transforms([b], [b["pos"]], [b["quat"]])[0], M, atol=1e-12)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_sweep_and_prune_pairs_equal_all_pairs(seed):
+    rng = np.random.default_rng(seed)
+    n = 300
+    lo = np.round(rng.uniform(0, 4, (n, 3)), 1)  # a coarse grid: ties and touching faces
+    hi = lo + np.round(rng.uniform(0, 0.6, (n, 3)), 1)
+    hi[::17] = lo[::17]  # degenerate (flat) boxes
+    static = rng.uniform(size=n) < 0.2
+    want = [(i, j) for i in range(n) for j in range(i + 1, n)
+            if not (static[i] and static[j]) and np.all(lo[i] <= hi[j]) and np.all(lo[j] <= hi[i])]
+    assert meshscene.overlapping_pairs(lo, hi, static) == want
+    assert meshscene.overlapping_pairs(lo[:1], hi[:1], static[:1]) == []
