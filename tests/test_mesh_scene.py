@@ -115,7 +115,7 @@ def test_mesh_fixture_regenerates_from_reference_files():
     # the full 128-link scene loads through the YAML path, link 0 static
     sc = yamlcfg.load_mesh_scene(os.path.join(REF, "scenes", "chain", "chain.yaml"))
     assert len(sc["bodies"]) == 128 and sc["bodies"][0]["is_static"] and not sc["bodies"][1]["is_static"]
-    # the bolt scene: a bolt and its static nut, only-normal force
+    # the bolt scene: two mesh bodies, body 1 static, only-normal force
     bolt = os.path.join(REF, "scenes", "bolt", "bolt.yaml")
     sc = yamlcfg.load_mesh_scene(bolt)
     assert [b["is_static"] for b in sc["bodies"]] == [False, True]
