@@ -217,10 +217,12 @@ class MeshScene:
         every overlapping pair's contacts from one pdc_mesh_contacts_pairs call."""
         pairs = self.pairs()
         pose = np.concatenate([self.pos, self.quat], 1)
-        c = self.lib.mesh_contacts_pairs([(self.meshes[i], pose[i], self.meshes[j], pose[j]) for i, j in pairs],
-                                         out=self.buffers)
-        if c["n"] > self.max_points:
-            raise RuntimeError(f"{c['n']} contact points, more than max_points = {self.max_points}")
+        query = [(self.meshes[i], pose[i], self.meshes[j], pose[j]) for i, j in pairs]
+        c = self.lib.mesh_contacts_pairs(query, out=self.buffers)
+        if c["n"] > self.max_points:  # more points than the buffers hold: grow them and ask again
+            self.max_points = 1 << (int(c["n"]) - 1).bit_length()
+            self.buffers = self.lib.mesh_contact_buffers(self.max_points)
+            c = self.lib.mesh_contacts_pairs(query, out=self.buffers)
         body = np.repeat(np.array(pairs, np.int32).reshape(-1, 2), c["counts"], axis=0)
         counts = list(zip(pairs, c["counts"].tolist()))
         R = _rotations(self.quat)

@@ -185,3 +185,75 @@ def test_sweep_and_prune_pairs_equal_all_pairs(seed):
             if not (static[i] and static[j]) and np.all(lo[i] <= hi[j]) and np.all(lo[j] <= hi[i])]
     assert meshscene.overlapping_pairs(lo, hi, static) == want
     assert meshscene.overlapping_pairs(lo[:1], hi[:1], static[:1]) == []
+
+
+def _restated_device(monkeypatch):
+    """MeshScene's device calls replaced by their CPU restatements (mesh
+    contacts: oracle/meshmesh_ref.py; solve: the oracle), to check its host
+    logic without a GPU."""
+    import meshmesh_ref as mm
+    import oracle_lib
+
+    from primal_dual_contacts_miror_b200 import lib
+
+    class RestatedMesh:
+        def __init__(self, v, f):
+            self.m = mm.Mesh(v, f)
+
+        def close(self):
+            pass
+
+    class RestatedSolver:
+        def __init__(self, cfg):
+            self.cfg = cfg
+
+        def solve(self, hs, dt, gravity):
+            return oracle_lib.solve(hs, dt=dt, gravity=gravity, cfg=self.cfg)
+
+        def close(self):
+            pass
+
+    def pairs(query, max_points=65536, out=None):
+        if out is not None:
+            max_points = len(out["pos"])
+        rows = [c for a, pa, b, pb in query for c in mm.contacts(a.m, pa[:3], pa[3:], b.m, pb[:3], pb[3:])]
+        counts = [len(mm.contacts(a.m, pa[:3], pa[3:], b.m, pb[:3], pb[3:])) for a, pa, b, pb in query]
+        k = min(len(rows), max_points)
+        shape = {"pos": 3, "normal": 3, "depth": None, "frame": 9, "arm": 6}
+        res = {}
+        for key, w in shape.items():
+            vals = [np.asarray(c[key]).reshape(-1) if w else c[key] for c in rows[:k]]
+            res[key] = np.array(vals, float).reshape((k, w) if w else (k,))
+        res["counts"], res["n"] = np.array(counts, np.int32), len(rows)
+        return res
+
+    monkeypatch.setattr(lib, "Mesh", RestatedMesh)
+    monkeypatch.setattr(lib, "Solver", RestatedSolver)
+    monkeypatch.setattr(lib, "mesh_contacts_pairs", pairs)
+
+
+def test_mesh_scene_host_logic_with_restated_device_calls(monkeypatch):
+    from primal_dual_contacts_miror_b200 import abi
+
+    _restated_device(monkeypatch)
+    floor = meshscene.mesh_body(np.eye(4), *meshes.box((1.0, 1.0, 0.1)), density=1000.0)
+    floor["is_static"] = True
+    M = np.eye(4)
+    M[:3, 3] = (0.0, 0.0, 0.1 + 0.2 - 0.002)
+    box = meshscene.mesh_body(M, *meshes.box((0.2, 0.2, 0.2)), density=500.0)
+    box["vel"] = (0.0, 0.0, -0.5)
+    bodies = [floor, box]
+    cfg = abi.default_config(tol=1e-8, mu=0.4)
+    g = (0.0, 0.0, -9.81)
+    scene = meshscene.MeshScene(bodies, 0.01, g, cfg=cfg, max_points=2)  # too small: the buffers grow
+    models = world_ref.mesh_models(bodies)
+    state = world_ref.mesh_initial_state(bodies)
+    for step in range(3):
+        scene.step(1)
+        st, hs = world_ref.mesh_step(bodies, models, state, 0.01, g, cfg)
+        assert scene.last_n_contacts == hs.n_contacts == 4, step  # the box's four bottom corners
+        for x, y in zip(scene.state(), state):
+            np.testing.assert_allclose(x, y, atol=1e-14)
+    assert scene.max_points == 4
+    n = scene.step_adaptive(2, 5.0)
+    assert len(n) == 2 and all(k >= 1 for k in n)
