@@ -125,8 +125,9 @@ def _boxes_intersect(ca, Ra, ha, cb, Rb, hb):
 def test_box_box_separation_and_points_on_random_pairs():
     """On random box pairs: no points exactly when the boxes do not meet (an
     independent vertex-inside / edge-crosses-face test); every point lies in
-    both boxes grown by half its depth, depth at most the least separating-axis
-    overlap, normal unit and from the first box towards the second."""
+    both boxes grown by half its depth, depth within the least separating-axis
+    overlap (over 0.95, the face-axis preference), normal unit and from the
+    first box towards the second."""
     rng = np.random.default_rng(7)
     met = 0
     for _ in range(250):
@@ -144,7 +145,8 @@ def test_box_box_separation_and_points_on_random_pairs():
                     - abs((cb - ca) @ L) for L in (x / np.linalg.norm(x) for x in axes if np.linalg.norm(x) > 1e-9))
         for p, n, d in pts:
             assert abs(np.linalg.norm(n) - 1.0) < 1e-12 and n @ (cb - ca) >= 0
-            assert -1e-12 <= d <= least + 1e-9
+            # face axes are preferred unless an edge axis overlaps 5 % less
+            assert -1e-12 <= d <= (least + 1e-9) / 0.95
             for c, R, h in ((ca, Ra, ha), (cb, Rb, hb)):
                 assert np.all(np.abs(R.T @ (p - c)) <= h + 0.5 * d + 1e-9)
     assert 60 < met < 240
